@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""RHS solves/s of the gpu_iterative Helmholtz path on B200.
+
+Workload (one "step" = one right-hand side solved to the scaled relative
+residual rtol): the 128^3 variable-medium scene at h = 1 mm, 40 kHz, seeded
+Gaussian random c and rho (sigma = 4 cells, +-3 clip), a rho=1250/c=2200
+blended sphere of radius 15 mm 60 mm above the baffle, +x reflecting wall,
+10-cell quadratic PML on the other open faces, 8 x 8 sinc_neumann array
+(radius 4.5 mm, pitch 10.5 mm), seeded phases. Inputs are synthetic.
+
+Our arm: mixed-precision GMRES (complex64 Krylov vectors, FP64 dots,
+Hessenberg/Givens, true residual and solution update at every restart) on
+the matrix-free sm_100a stencil; the plain FP64 GMRES of the same stencil is
+timed once beside it, and the relative L2 difference between the two
+solutions is reported. `--impl reference` times the reference's CPU
+algorithm (the oracle's restatement: CSR assembly + row-scaled Jacobi GMRES
+in scipy/numpy) on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "RHS solves/s at 128^3 (config-1 scene), mixed-precision GMRES, rel err <=1e-6 vs FP64"
+UNIT = "RHS solves/s"
+FALLBACK_HBM_GBS = 6650.0
+# Inner iterations the row-scaled Jacobi GMRES(112) needs on this scene to
+# reach rtol 1e-9 (FP64 arm of this bench on a B200); the CPU sample below is
+# converted to solves/s with it because a full CPU solve takes hours.
+ITERATIONS_PER_SOLVE_FP64 = 30016
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--restart", type=int, default=112)
+    ap.add_argument("--rtol", type=float, default=1e-9)
+    ap.add_argument("--maxiter", type=int, default=60000)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GMRES comparator")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=20)
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------- distributed
+def dist_setup(n_gpus):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- workload
+def workload_config(args):
+    from ultrasound_solver_b200 import workloads as W
+    cfg = W.config1(n=args.grid)
+    desc = {"workload": f"config-1 scene: {args.grid}^3 nodes h=1mm 40kHz, random c/rho "
+                        "(sigma 4 cells), r=15mm rho=1250 sphere blended, +x reflecting, "
+                        "10-cell quadratic PML, 8x8 sinc_neumann array, 1 RHS per step",
+            "grid": [args.grid] * 3, "nodes": args.grid ** 3, "restart": args.restart,
+            "rtol": args.rtol, "precision": "complex64 Krylov + FP64 refinement",
+            "l2": "inputs larger than L2 (Krylov basis %.1f GB)" % (
+                (args.restart + 1) * args.grid ** 3 * 8 / 1e9),
+            "parallelism": "replicas (independent RHS per GPU)"}
+    return cfg, desc
+
+
+def run_ours(args):
+    import torch
+
+    from ultrasound_solver_b200 import workloads as W
+
+    rank, world, local = dist_setup(args.gpus)
+    cfg, desc = workload_config(args)
+    solver = W.build_solver(cfg, seed=0)
+    rng = np.random.default_rng(1 + rank)
+    solver.set_phases(rng.uniform(0, 2 * np.pi, solver.transducers.num_transducers))
+    solver.assemble_matrix()
+    rhs = solver.update_rhs_device()
+    it = solver.iterative_solver
+    it.restart, it.rtol, it.maxiter = args.restart, args.rtol, args.maxiter
+    it.backward_error_tol = 1e-4
+    stream = torch.cuda.current_stream()
+
+    def solve(precision, profile=False):
+        it.precision, it.profile = precision, profile
+        return it.solve(solver.operator, rhs)
+
+    # warm-up (untimed)
+    for _ in range(args.warmup):
+        x_mixed = solve("mixed")
+    torch.cuda.synchronize()
+    # timed region: K solves from device-resident inputs
+    barrier(world)
+    torch.cuda.synchronize()
+    prof_tot = {}
+    launches = 0
+    iterations = []
+    with ClockSampler(local) as clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            x_mixed = solve("mixed", profile=True)
+            iterations.append(it.last_iterations)
+            for name, d in it.last_profile.items():
+                agg = prof_tot.setdefault(name, dict(launches=0, ms=0.0, bytes=0.0))
+                for k in agg:
+                    agg[k] += d[k]
+            launches += sum(d["launches"] for d in it.last_profile.values()) + 1
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_local = start.elapsed_time(stop)
+    ms = max_over_ranks(ms_local, world)
+    value = world * args.steps / (ms / 1000.0)
+    stats = dict(it.last_stats[0])
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "c64+f64", "data": "synthetic", "config": desc,
+           "iterations_per_solve": iterations, "scaled_residual": stats["scaled_residual"],
+           "backward_error": stats["backward_error"]}
+    out["clocks"] = clocks.summary()
+    out["gpu_launches"] = launches
+
+    # roofline of the dominant kernel family (live CUDA-event timing)
+    peak, peak_kind = measured_peak()
+    dom = max(prof_tot, key=lambda k: prof_tot[k]["ms"])
+    d = prof_tot[dom]
+    achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9 if d["ms"] > 0 else None
+    out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                       "peak_source": peak_kind, "unit": "GB/s",
+                       "frac": achieved / peak if achieved else None,
+                       "traffic": None,
+                       "avg_launch_us": 1000.0 * d["ms"] / max(d["launches"], 1),
+                       "algorithmic_bytes_per_launch": d["bytes"] / max(d["launches"], 1),
+                       "families": {k: {"launches": v["launches"], "ms": v["ms"],
+                                        "GBps": (v["bytes"] / (v["ms"] / 1e3) / 1e9)
+                                        if v["ms"] > 0 and v["bytes"] > 0 else None}
+                                    for k, v in prof_tot.items()}}
+
+    # plain FP64 GMRES of the same stencil (comparator) + parity of the two fields
+    if not args.no_fp64:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        x64 = solve("fp64")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        rel = float((torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item())
+        out["fp64_gmres"] = {"solves_per_s": 1000.0 / ms64, "ms_per_solve": ms64,
+                             "iterations": it.last_iterations,
+                             "speedup_mixed_vs_fp64": (value / world) / (1000.0 / ms64)}
+        out["rel_err_vs_fp64"] = rel
+
+    # end to end through the public API with host buffers
+    if not args.no_e2e:
+        it.precision, it.profile = "mixed", False
+        rhs_host = rhs.cpu().numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_e2e = max(1, min(args.steps, 2))
+        for _ in range(n_e2e):
+            xh = solver.solve_rhs(rhs_host, verbose=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        e2e = max_over_ranks(dt, world)
+        out["e2e"] = {"value": world * n_e2e / e2e, "unit": UNIT,
+                      "h2d_bytes_per_step": int(rhs_host.nbytes),
+                      "d2h_bytes_per_step": int(xh.nbytes), "steps": n_e2e,
+                      "api": "HelmholtzB200Solver.solve_rhs(numpy)"}
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_sample(args, cfg)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_scene(args, cfg):
+    """The same scene assembled by the oracle's restatement of the reference."""
+    from oracle import helmholtz_oracle as O
+    from ultrasound_solver_b200 import workloads as W
+    n = args.grid
+    shape = (n,) * 3
+    dx = cfg["domain"]["box_size"][0] / (n - 1)
+    rho_m, c_m = W.random_medium(shape, 0)
+    ob = cfg["obstacles"][0]
+    h = O.smoothed_heaviside(O.sphere_sdf(shape, dx, ob["center"], ob["radius"]), 1.2 * dx)
+    rho, c = O.blend_obstacle_material(h, 1250.0, 2200.0, rho_m, c_m)
+    c2 = dict(cfg)
+    c2["obstacles"] = []
+    m = cfg["transducer_specs"]["array_n"] ** 2
+    phases = np.random.default_rng(1).uniform(0, 2 * np.pi, m)
+    return O.build_scene(c2, material_fields=(rho, c), phases=phases)
+
+
+def cpu_iterations_per_second(args, sc, iters):
+    """Time `iters` Arnoldi steps of the restated row-scaled Jacobi GMRES."""
+    from oracle import helmholtz_oracle as O
+    A = sc.A
+    R, inv_d = O.row_scale_and_jacobi(A)
+    b = R * sc.rhs
+    m = min(args.restart, iters)
+    t0 = time.perf_counter()
+    # one truncated cycle of the restated algorithm: m steps of CGS Arnoldi
+    r = b.copy()
+    beta = np.linalg.norm(r)
+    V = np.empty((len(b), m + 1), dtype=np.complex128)
+    V[:, 0] = r / beta
+    for j in range(m):
+        u = R * (A @ (inv_d * V[:, j]))
+        h = V[:, :j + 1].conj().T @ u
+        u = u - V[:, :j + 1] @ h
+        V[:, j + 1] = u / np.linalg.norm(u)
+    dt = time.perf_counter() - t0
+    return m / dt, m, dt
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads", 1) for i in threadpool_info() if i.get("user_api") == "blas"]
+        return max(n) if n else 1
+    except Exception:
+        return 1
+
+
+def cpu_sample(args, cfg):
+    sc = cpu_scene(args, cfg)
+    its, m, dt = cpu_iterations_per_second(args, sc, args.cpu_iters)
+    return {"value": its / ITERATIONS_PER_SOLVE_FP64, "unit": UNIT, "cores": blas_threads(),
+            "kind": "port",
+            "sample": (f"{m} Arnoldi steps of the restated row-scaled Jacobi GMRES({args.restart}) "
+                       f"on the {args.grid}^3 scene in {dt:.1f}s ({its:.2f} it/s, scipy CSR SpMV "
+                       f"single-threaded); solves/s = it/s / {ITERATIONS_PER_SOLVE_FP64} "
+                       "iterations per solve")}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg, desc = workload_config(args)
+    sc = cpu_scene(args, cfg)
+    for _ in range(args.warmup):
+        cpu_iterations_per_second(args, sc, 4)
+    t0 = time.perf_counter()
+    total_it = 0
+    for _ in range(args.steps):
+        its, m, dt = cpu_iterations_per_second(args, sc, args.cpu_iters)
+        total_it += m
+    dt = time.perf_counter() - t0
+    its = total_it / dt
+    value = its / ITERATIONS_PER_SOLVE_FP64
+    cores = blas_threads()
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+           "data": "synthetic", "config": desc, "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                            "sample": (f"{args.cpu_iters} Arnoldi steps per step of the restated "
+                                       f"row-scaled Jacobi GMRES({args.restart}) (reference CPU "
+                                       f"algorithm, CuPy gmres restated in numpy/scipy); "
+                                       f"{its:.3f} it/s; solves/s = it/s / "
+                                       f"{ITERATIONS_PER_SOLVE_FP64} iterations per solve")},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

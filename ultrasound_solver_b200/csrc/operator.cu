@@ -1,0 +1,393 @@
+// Operator set-up and application: per-node coefficient records built on the
+// device from rho and c, and the matrix-free 7-point apply kernels.
+//
+// Parity: the diagonal, edge coefficients and face terms follow
+// ConservativeHelmholtz (src/algorithm/physics/conservative_helmholtz.py:36-149);
+// R = 1/max|row| and s = 1/(R A_ii) follow GpuIterativeSolver.solve
+// (src/algorithm/solvers/iterative_solver.py:37-56), for A and for A^H.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "usv_internal.cuh"
+
+namespace usv {
+
+static thread_local cudaError_t g_last_cuda = cudaSuccess;
+int set_last_cuda_error(cudaError_t e) {
+    g_last_cuda = e;
+    return USV_ERR_CUDA;
+}
+
+// ------------------------------------------------------------ 1-D tables
+// Half-volume weights w and PML stretch s = 1 + i sigma per axis
+// (conservative_helmholtz.py:48-64), folded into T = w s and
+// Q = 1/(0.5 (s_i + s_{i+1}) dx^2).
+struct AxisTables {
+    std::vector<double2> T, Q;
+};
+
+static int validate_scene(const usv_scene& s) {
+    if (s.nx < 2 || s.ny < 2 || s.nz < 2) return USV_ERR_ARG;
+    if (!(std::isfinite(s.dx) && s.dx > 0 && std::isfinite(s.omega) && s.omega > 0))
+        return USV_ERR_ARG;
+    for (int f = 0; f < 6; ++f) {
+        int k = s.face_kind[f];
+        if (k < USV_FACE_REFLECTING || k > USV_FACE_IMPEDANCE) return USV_ERR_ARG;
+        if (k == USV_FACE_IMPEDANCE) {
+            double zr = s.impedance_re[f], zi = s.impedance_im[f];
+            if (!std::isfinite(zr) || !std::isfinite(zi) || zr < 0 || (zr == 0 && zi == 0))
+                return USV_ERR_ARG;
+        }
+    }
+    if (s.pml_cells < 0 || s.pml_order < 1 || !(s.pml_strength >= 0) ||
+        !std::isfinite(s.pml_strength))
+        return USV_ERR_ARG;
+    if (s.pml_faces & ~0x3f) return USV_ERR_ARG;
+    const int dims[3] = {s.nx, s.ny, s.nz};
+    for (int a = 0; a < 3; ++a) {
+        int active = 0;
+        for (int side = 0; side < 2; ++side)
+            if (s.pml_faces & (1 << (2 * a + side))) ++active;
+        if (s.pml_cells && active) {
+            if ((long long)s.pml_cells * active >= dims[a] - 1) return USV_ERR_ARG;
+            for (int side = 0; side < 2; ++side)
+                if ((s.pml_faces & (1 << (2 * a + side))) &&
+                    s.face_kind[2 * a + side] != USV_FACE_OPEN)
+                    return USV_ERR_ARG;
+        }
+    }
+    return USV_OK;
+}
+
+static AxisTables axis_tables(const usv_scene& s, int axis) {
+    const int dims[3] = {s.nx, s.ny, s.nz};
+    const int n = dims[axis];
+    std::vector<double> w(n, 1.0), sigma(n, 0.0);
+    w[0] = w[n - 1] = 0.5;
+    if (s.pml_cells > 0) {
+        for (int side = 0; side < 2; ++side) {
+            if (!(s.pml_faces & (1 << (2 * axis + side)))) continue;
+            for (int i = 0; i < n; ++i) {
+                double dist = side == 0 ? double(i) : double(n - 1 - i);
+                double t = 1.0 - dist / double(s.pml_cells);
+                if (t > 0) sigma[i] += s.pml_strength * std::pow(t, double(s.pml_order));
+            }
+        }
+    }
+    AxisTables t;
+    t.T.resize(n);
+    t.Q.resize(n);
+    const double dx2 = s.dx * s.dx;
+    for (int i = 0; i < n; ++i) t.T[i] = make_double2(w[i], w[i] * sigma[i]);
+    for (int i = 0; i < n; ++i) {
+        if (i + 1 < n) {
+            double2 mid = make_double2(1.0, 0.5 * (sigma[i] + sigma[i + 1]));
+            t.Q[i] = cinv(make_double2(mid.x * dx2, mid.y * dx2));
+        } else {
+            t.Q[i] = make_double2(0.0, 0.0);
+        }
+    }
+    return t;
+}
+
+// ------------------------------------------------------------ build kernel
+struct BuildArgs {
+    OpView<double> op;      // tables + output records (cast away const below)
+    const double* rho;
+    const double* c;
+    double omega, dx;
+    int face_kind[6];
+    double2 face_adm[6];    // 1/Z for impedance faces
+    double4* rec64f;
+    double4* rec64a;
+    double2* d64;
+    float4* rec32f;
+    float4* rec32a;
+    int* flag;
+};
+
+__global__ void __launch_bounds__(256) k_build(BuildArgs a) {
+    const OpView<double>& op = a.op;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
+         n += (long long)gridDim.x * blockDim.x) {
+        const Node p = decode(n, op.nx, op.ny);
+        const double rho = a.rho[n], c = a.c[n];
+        if (!(rho > 0) || !(c > 0) || !isfinite(rho) || !isfinite(c)) atomicOr(a.flag, 1);
+        const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
+        const double2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
+        // mass term: w_x w_y w_z s_x s_y s_z omega^2 / (rho c^2)
+        double2 diag = cscale(cmul(cmul(tx, ty), tz), a.omega * a.omega / (rho * c * c));
+        double emax_all = 0.0, emax_free = 0.0;
+        const double2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
+        auto edge = [&](long long m, double2 F, bool nb_fixed) {
+            const double g = 2.0 / (rho + a.rho[m]);
+            const double2 e = cscale(F, g);
+            diag = csub(diag, e);
+            const double ae = hypot(e.x, e.y);
+            emax_all = fmax(emax_all, ae);
+            if (!nb_fixed) emax_free = fmax(emax_free, ae);
+        };
+        const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+        if (p.i > 0)
+            edge(n - 1, cmul(fyz, op.Q[0][p.i - 1]),
+                 node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
+        if (p.i < op.nx - 1)
+            edge(n + 1, cmul(fyz, op.Q[0][p.i]),
+                 node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
+        if (p.j > 0)
+            edge(n - sy, cmul(fxz, op.Q[1][p.j - 1]),
+                 node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
+        if (p.j < op.ny - 1)
+            edge(n + sy, cmul(fxz, op.Q[1][p.j]),
+                 node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
+        if (p.k > 0)
+            edge(n - sz, cmul(fxy, op.Q[2][p.k - 1]),
+                 node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
+        if (p.k < op.nz - 1)
+            edge(n + sz, cmul(fxy, op.Q[2][p.k]),
+                 node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
+        // face terms i omega * area * admittance (conservative_helmholtz.py:89-103)
+        const int coord[3] = {p.i, p.j, p.k};
+        const int dims[3] = {op.nx, op.ny, op.nz};
+        for (int f = 0; f < 6; ++f) {
+            const int kind = a.face_kind[f];
+            if (kind != USV_FACE_OPEN && kind != USV_FACE_IMPEDANCE) continue;
+            const int axis = f >> 1;
+            if (coord[axis] != ((f & 1) ? dims[axis] - 1 : 0)) continue;
+            double2 area;
+            if (axis == 0) area = fyz;
+            else if (axis == 1) area = fxz;
+            else area = fxy;
+            area = cscale(area, 1.0 / a.dx);
+            const double2 adm = kind == USV_FACE_OPEN ? make_double2(1.0 / (rho * c), 0.0)
+                                                      : a.face_adm[f];
+            const double2 term = cmul(make_double2(0.0, a.omega), cmul(area, adm));
+            diag = cadd(diag, term);
+        }
+        if (fixed) diag = make_double2(1.0, 0.0);
+        const double adiag = hypot(diag.x, diag.y);
+        // forward: row maxima of |A| (fixed rows keep only the unit diagonal)
+        const double rowmax = fixed ? 1.0 : fmax(adiag, emax_all);
+        const double R = rowmax > 0 ? 1.0 / rowmax : 1.0;
+        const double2 sd = cscale(diag, R);
+        const double2 s = (sd.x != 0 || sd.y != 0) ? cinv(sd) : make_double2(1.0, 0.0);
+        // adjoint: row maxima of |A^H| = column maxima of |A|
+        const double colmax = fmax(adiag, emax_free);
+        const double Ra = colmax > 0 ? 1.0 / colmax : 1.0;
+        const double2 sda = cscale(cconj(diag), Ra);
+        const double2 sa = (sda.x != 0 || sda.y != 0) ? cinv(sda) : make_double2(1.0, 0.0);
+        a.rec64f[n] = make_double4(rho, R, s.x, s.y);
+        a.rec64a[n] = make_double4(rho, Ra, sa.x, sa.y);
+        a.d64[n] = diag;
+        a.rec32f[n] = make_float4(float(rho), float(R), float(s.x), float(s.y));
+        a.rec32a[n] = make_float4(float(rho), float(Ra), float(sa.x), float(sa.y));
+        if (!isfinite(diag.x) || !isfinite(diag.y)) atomicOr(a.flag, 2);
+    }
+}
+
+static unsigned grid_for(long long n, int threads = 256) {
+    long long b = (n + threads - 1) / threads;
+    if (b > 148LL * 32) b = 148LL * 32;
+    if (b < 1) b = 1;
+    return unsigned(b);
+}
+
+// ------------------------------------------------------------ apply kernels
+template <int VARIANT>
+__global__ void __launch_bounds__(256) k_apply_fp64(OpView<double> op, const double2* x,
+                                                    double2* y, long long ld) {
+    const int b = blockIdx.y;
+    const double2* xb = x + b * ld;
+    double2* yb = y + b * ld;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
+         n += (long long)gridDim.x * blockDim.x) {
+        yb[n] = a_row<VARIANT>(op, xb, n, decode(n, op.nx, op.ny));
+    }
+}
+
+template <typename R, bool ADJ>
+__global__ void __launch_bounds__(256) k_apply_k(OpView<R> op, const typename Tr<R>::c2* x,
+                                                 typename Tr<R>::c2* y, long long ld) {
+    const int b = blockIdx.y;
+    const auto* xb = x + b * ld;
+    auto* yb = y + b * ld;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
+         n += (long long)gridDim.x * blockDim.x) {
+        yb[n] = k_row<R, ADJ>(op, xb, n, decode(n, op.nx, op.ny));
+    }
+}
+
+__global__ void k_export(OpView<double> f, OpView<double> a, double* diag, double* rs,
+                         double* jac, double* rsa, double* jaca) {
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < f.n;
+         n += (long long)gridDim.x * blockDim.x) {
+        if (diag) { diag[2 * n] = f.d[n].x; diag[2 * n + 1] = f.d[n].y; }
+        if (rs) rs[n] = f.rec[n].y;
+        if (jac) { jac[2 * n] = f.rec[n].z; jac[2 * n + 1] = f.rec[n].w; }
+        if (rsa) rsa[n] = a.rec[n].y;
+        if (jaca) { jaca[2 * n] = a.rec[n].z; jaca[2 * n + 1] = a.rec[n].w; }
+    }
+}
+
+}  // namespace usv
+
+using namespace usv;
+
+extern "C" {
+
+int usv_abi_version(void) { return USV_ABI_VERSION; }
+
+const char* usv_status_string(int status) {
+    switch (status) {
+        case USV_OK: return "ok";
+        case USV_ERR_ARG: return "invalid argument";
+        case USV_ERR_CUDA: return cudaGetErrorString(g_last_cuda);
+        case USV_ERR_WORKSPACE: return "workspace too small";
+        case USV_ERR_NOT_CONVERGED: return "GMRES did not converge";
+        case USV_ERR_NONFINITE: return "non-finite value";
+        case USV_ERR_SOURCE_PML: return "PML overlaps the deposited sinc aperture";
+        case USV_ERR_SOURCE_SOFT: return "Sinc flux conflicts with a pressure-release boundary";
+        case USV_ERR_SOURCE_CLEARANCE:
+            return "Sinc aperture needs one grid cell clearance from side boundaries";
+        default: return "unknown status";
+    }
+}
+
+int usv_device_info(int* sm_count, int* cc_major, int* cc_minor) {
+    int dev = 0;
+    USV_CUDA_TRY(cudaGetDevice(&dev));
+    if (sm_count) USV_CUDA_TRY(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
+    if (cc_major) USV_CUDA_TRY(cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (cc_minor) USV_CUDA_TRY(cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
+    return USV_OK;
+}
+
+int usv_operator_bytes(const usv_scene* scene, size_t* bytes) {
+    if (!scene || !bytes) return USV_ERR_ARG;
+    int st = validate_scene(*scene);
+    if (st) return st;
+    *bytes = make_layout(*scene).total;
+    return USV_OK;
+}
+
+int usv_operator_build(const usv_scene* scene, const double* rho, const double* c,
+                       void* op_buf, size_t op_bytes, void* stream) {
+    if (!scene || !rho || !c || !op_buf) return USV_ERR_ARG;
+    const usv_scene& s = *scene;
+    int st = validate_scene(s);
+    if (st) return st;
+    const Layout L = make_layout(s);
+    if (op_bytes < L.total) return USV_ERR_WORKSPACE;
+    cudaStream_t strm = static_cast<cudaStream_t>(stream);
+    char* buf = static_cast<char*>(op_buf);
+    for (int a = 0; a < 3; ++a) {
+        AxisTables t = axis_tables(s, a);
+        const size_t n = t.T.size();
+        std::vector<float2> T32(n), Q32(n);
+        for (size_t i = 0; i < n; ++i) {
+            T32[i] = make_float2(float(t.T[i].x), float(t.T[i].y));
+            Q32[i] = make_float2(float(t.Q[i].x), float(t.Q[i].y));
+        }
+        USV_CUDA_TRY(cudaMemcpyAsync(buf + L.tab64[a], t.T.data(), n * sizeof(double2),
+                                     cudaMemcpyHostToDevice, strm));
+        USV_CUDA_TRY(cudaMemcpyAsync(buf + L.q64[a], t.Q.data(), n * sizeof(double2),
+                                     cudaMemcpyHostToDevice, strm));
+        USV_CUDA_TRY(cudaMemcpyAsync(buf + L.tab32[a], T32.data(), n * sizeof(float2),
+                                     cudaMemcpyHostToDevice, strm));
+        USV_CUDA_TRY(cudaMemcpyAsync(buf + L.q32[a], Q32.data(), n * sizeof(float2),
+                                     cudaMemcpyHostToDevice, strm));
+        // the host vectors die at scope end: finish the copies first
+        USV_CUDA_TRY(cudaStreamSynchronize(strm));
+    }
+    USV_CUDA_TRY(cudaMemsetAsync(buf + L.flag, 0, 64, strm));
+    BuildArgs a{};
+    a.op = make_view<double>(s, op_buf, false);
+    a.rho = rho;
+    a.c = c;
+    a.omega = s.omega;
+    a.dx = s.dx;
+    for (int f = 0; f < 6; ++f) {
+        a.face_kind[f] = s.face_kind[f];
+        a.face_adm[f] = s.face_kind[f] == USV_FACE_IMPEDANCE
+                            ? cinv(make_double2(s.impedance_re[f], s.impedance_im[f]))
+                            : make_double2(0.0, 0.0);
+    }
+    a.rec64f = reinterpret_cast<double4*>(buf + L.rec64f);
+    a.rec64a = reinterpret_cast<double4*>(buf + L.rec64a);
+    a.d64 = reinterpret_cast<double2*>(buf + L.d64);
+    a.rec32f = reinterpret_cast<float4*>(buf + L.rec32f);
+    a.rec32a = reinterpret_cast<float4*>(buf + L.rec32a);
+    a.flag = reinterpret_cast<int*>(buf + L.flag);
+    k_build<<<grid_for(a.op.n), 256, 0, strm>>>(a);
+    USV_CUDA_TRY(cudaGetLastError());
+    int flag = 0;
+    USV_CUDA_TRY(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, strm));
+    USV_CUDA_TRY(cudaStreamSynchronize(strm));
+    if (flag & 1) return USV_ERR_ARG;
+    if (flag & 2) return USV_ERR_NONFINITE;
+    return USV_OK;
+}
+
+int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant, int precision,
+                       const void* x, void* y, int nrhs, int64_t ld, void* stream) {
+    if (!scene || !op_buf || !x || !y || nrhs < 1 || nrhs > 65535) return USV_ERR_ARG;
+    const usv_scene& s = *scene;
+    const long long n = (long long)s.nx * s.ny * s.nz;
+    if (ld < n) return USV_ERR_ARG;
+    cudaStream_t strm = static_cast<cudaStream_t>(stream);
+    dim3 grid(grid_for(n), nrhs);
+    switch (variant) {
+        case USV_APPLY_A:
+            k_apply_fp64<USV_APPLY_A><<<grid, 256, 0, strm>>>(
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+            break;
+        case USV_APPLY_AH:
+            k_apply_fp64<USV_APPLY_AH><<<grid, 256, 0, strm>>>(
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+            break;
+        case USV_APPLY_ABS_A:
+            k_apply_fp64<USV_APPLY_ABS_A><<<grid, 256, 0, strm>>>(
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+            break;
+        case USV_APPLY_ABS_AH:
+            k_apply_fp64<USV_APPLY_ABS_AH><<<grid, 256, 0, strm>>>(
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+            break;
+        case USV_APPLY_K:
+        case USV_APPLY_KH: {
+            const bool adj = variant == USV_APPLY_KH;
+            if (precision == USV_PREC_FP64) {
+                auto v = make_view<double>(s, op_buf, adj);
+                if (adj) k_apply_k<double, true><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld);
+                else k_apply_k<double, false><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld);
+            } else if (precision == USV_PREC_MIXED) {
+                auto v = make_view<float>(s, op_buf, adj);
+                if (adj) k_apply_k<float, true><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld);
+                else k_apply_k<float, false><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld);
+            } else {
+                return USV_ERR_ARG;
+            }
+            break;
+        }
+        default:
+            return USV_ERR_ARG;
+    }
+    USV_CUDA_TRY(cudaGetLastError());
+    return USV_OK;
+}
+
+int usv_operator_export(const usv_scene* scene, const void* op_buf, double* diag,
+                        double* row_scale, double* jacobi, double* row_scale_adj,
+                        double* jacobi_adj, void* stream) {
+    if (!scene || !op_buf) return USV_ERR_ARG;
+    const usv_scene& s = *scene;
+    auto f = make_view<double>(s, op_buf, false);
+    auto a = make_view<double>(s, op_buf, true);
+    k_export<<<grid_for(f.n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        f, a, diag, row_scale, jacobi, row_scale_adj, jacobi_adj);
+    USV_CUDA_TRY(cudaGetLastError());
+    return USV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,311 @@
+// Internal device/host helpers of the sm_100a Helmholtz backend.
+//
+// The operator is matrix-free. Instead of the reference's CSR matrix
+// (conservative_helmholtz.py:119-149, ~7 nnz/row, ~176 B/row) each node keeps
+// one record {rho, R, s.re, s.im}: the density (edge coefficients are formed
+// on the fly as F * 2/(rho_i + rho_j), F from 1-D PML tables), the row scale
+// R = 1/max|row| and the Jacobi factor s = 1/(R A_ii) of the reference's
+// row-scaled Jacobi GMRES (iterative_solver.py:37-56). A second record holds
+// the same for A^H (column maxima), and an fp64 array holds the diagonal A_ii
+// for the unscaled residual. Fixed (soft-face) rows are recognised from the
+// node coordinates, so no mask is stored.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "usv.h"
+
+namespace usv {
+
+// ---------------------------------------------------------------- types
+template <typename R> struct Tr;
+template <> struct Tr<float> {
+    using c2 = float2;
+    using c4 = float4;
+};
+template <> struct Tr<double> {
+    using c2 = double2;
+    using c4 = double4;
+};
+
+template <typename C> __host__ __device__ __forceinline__ C cmake(double re, double im);
+template <> __host__ __device__ __forceinline__ float2 cmake<float2>(double re, double im) {
+    return make_float2(float(re), float(im));
+}
+template <> __host__ __device__ __forceinline__ double2 cmake<double2>(double re, double im) {
+    return make_double2(re, im);
+}
+
+template <typename C, typename S> __host__ __device__ __forceinline__ C make_c2(S re, S im) {
+    C r; r.x = re; r.y = im; return r;
+}
+
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) {
+    C r; r.x = a.x + b.x; r.y = a.y + b.y; return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) {
+    C r; r.x = a.x - b.x; r.y = a.y - b.y; return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+    C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+// conj(a) * b
+template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
+    C r; r.x = a.x * b.x + a.y * b.y; r.y = a.x * b.y - a.y * b.x; return r;
+}
+template <typename C, typename S> __host__ __device__ __forceinline__ C cscale(C a, S s) {
+    C r; r.x = a.x * s; r.y = a.y * s; return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) {
+    C r; r.x = a.x; r.y = -a.y; return r;
+}
+__host__ __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__host__ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double cabs(double2 a) { return hypot(a.x, a.y); }
+__device__ __forceinline__ float cabs(float2 a) { return hypotf(a.x, a.y); }
+__host__ __device__ __forceinline__ double2 cinv(double2 a) {
+    double d = a.x * a.x + a.y * a.y;
+    return make_double2(a.x / d, -a.y / d);
+}
+__device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
+template <typename C> __device__ __forceinline__ C from_d(double2 a);
+template <> __device__ __forceinline__ float2 from_d<float2>(double2 a) {
+    return make_float2(float(a.x), float(a.y));
+}
+template <> __device__ __forceinline__ double2 from_d<double2>(double2 a) { return a; }
+
+// ---------------------------------------------------------------- layout
+// Byte offsets of the operator buffer. Everything is derived from the scene,
+// so host and device agree without storing the layout itself.
+struct Layout {
+    size_t tab64[3], q64[3], tab32[3], q32[3];
+    size_t rec64f, rec64a, d64, rec32f, rec32a, flag;
+    size_t total;
+};
+
+inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+inline Layout make_layout(const usv_scene& s) {
+    Layout L{};
+    const size_t n = size_t(s.nx) * size_t(s.ny) * size_t(s.nz);
+    const int dims[3] = {s.nx, s.ny, s.nz};
+    size_t off = 0;
+    for (int a = 0; a < 3; ++a) {
+        L.tab64[a] = off; off = align_up(off + sizeof(double2) * dims[a]);
+        L.q64[a] = off;   off = align_up(off + sizeof(double2) * dims[a]);
+        L.tab32[a] = off; off = align_up(off + sizeof(float2) * dims[a]);
+        L.q32[a] = off;   off = align_up(off + sizeof(float2) * dims[a]);
+    }
+    L.rec64f = off; off = align_up(off + sizeof(double4) * n);
+    L.rec64a = off; off = align_up(off + sizeof(double4) * n);
+    L.d64 = off;    off = align_up(off + sizeof(double2) * n);
+    L.rec32f = off; off = align_up(off + sizeof(float4) * n);
+    L.rec32a = off; off = align_up(off + sizeof(float4) * n);
+    L.flag = off;   off = align_up(off + 64);
+    L.total = off;
+    return L;
+}
+
+// Kernel-side view of one operator in precision R (float: complex64 path,
+// double: complex128 path).
+template <typename R> struct OpView {
+    using C2 = typename Tr<R>::c2;
+    using C4 = typename Tr<R>::c4;
+    int nx, ny, nz;
+    long long n;
+    unsigned soft;          // bit f: face f is a pressure-release face
+    const C2* T[3];         // T_a[i] = w_a[i] * s_a[i]
+    const C2* Q[3];         // Q_a[i] = 1 / (0.5 (s_a[i] + s_a[i+1]) dx^2)
+    const C4* rec;          // {rho, R, s.re, s.im} (forward or adjoint)
+    const double2* d;       // diagonal A_ii (fp64 path only)
+};
+
+inline unsigned soft_mask(const usv_scene& s) {
+    unsigned m = 0;
+    for (int f = 0; f < 6; ++f)
+        if (s.face_kind[f] == USV_FACE_SOFT) m |= 1u << f;
+    return m;
+}
+
+template <typename R>
+inline OpView<R> make_view(const usv_scene& s, const void* buf, bool adjoint) {
+    Layout L = make_layout(s);
+    const char* b = static_cast<const char*>(buf);
+    OpView<R> v{};
+    v.nx = s.nx; v.ny = s.ny; v.nz = s.nz;
+    v.n = (long long)s.nx * s.ny * s.nz;
+    v.soft = soft_mask(s);
+    const bool dbl = sizeof(R) == 8;
+    for (int a = 0; a < 3; ++a) {
+        v.T[a] = reinterpret_cast<const typename OpView<R>::C2*>(b + (dbl ? L.tab64[a] : L.tab32[a]));
+        v.Q[a] = reinterpret_cast<const typename OpView<R>::C2*>(b + (dbl ? L.q64[a] : L.q32[a]));
+    }
+    size_t rec = dbl ? (adjoint ? L.rec64a : L.rec64f) : (adjoint ? L.rec32a : L.rec32f);
+    v.rec = reinterpret_cast<const typename OpView<R>::C4*>(b + rec);
+    v.d = reinterpret_cast<const double2*>(b + L.d64);
+    return v;
+}
+
+// ---------------------------------------------------------------- nodes
+__device__ __forceinline__ bool node_fixed(unsigned soft, int i, int j, int k, int nx, int ny,
+                                           int nz) {
+    return ((soft & 1u) && i == 0) || ((soft & 2u) && i == nx - 1) ||
+           ((soft & 4u) && j == 0) || ((soft & 8u) && j == ny - 1) ||
+           ((soft & 16u) && k == 0) || ((soft & 32u) && k == nz - 1);
+}
+
+struct Node {
+    int i, j, k;
+};
+
+__device__ __forceinline__ Node decode(long long n, int nx, int ny) {
+    long long t = n / nx;
+    Node p;
+    p.i = int(n - t * nx);
+    p.k = int(t / ny);
+    p.j = int(t - (long long)p.k * ny);
+    return p;
+}
+
+// Row of the row-scaled Jacobi operator K = R A S (forward) or
+// K' = R' A^H S' (adjoint) at node n, applied to u (scaled by `scale`):
+//   forward : y = u_n + R_n sum_j e_nj s_j u_j          (fixed row: y = u_n)
+//   adjoint : y = u_n + R'_n sum_{j not fixed} conj(e_nj) s'_j u_j
+// The unit diagonal follows from s = 1/(R A_ii) (iterative_solver.py:46-56).
+template <typename R, bool ADJ>
+__device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op,
+                                                    const typename Tr<R>::c2* __restrict__ u,
+                                                    long long n, Node p) {
+    using C2 = typename Tr<R>::c2;
+    using C4 = typename Tr<R>::c4;
+    const C2 un = u[n];
+    const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
+    if (!ADJ && fixed) return un;
+    const C4 me = op.rec[n];
+    const C2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
+    const C2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
+    C2 acc = cmake<C2>(0.0, 0.0);
+    auto edge = [&](long long m, C2 F, bool nb_fixed) {
+        if (ADJ && nb_fixed) return;
+        const C4 r = op.rec[m];
+        const R g = R(2) / (me.x + r.x);
+        C2 e = cscale(F, g);
+        if (ADJ) e = cconj(e);
+        C2 sv = cmul(make_c2<C2>(r.z, r.w), u[m]);
+        acc = cadd(acc, cmul(e, sv));
+    };
+    const long long sx = 1, sy = op.nx, sz = (long long)op.nx * op.ny;
+    if (p.i > 0)
+        edge(n - sx, cmul(fyz, op.Q[0][p.i - 1]),
+             ADJ && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.i < op.nx - 1)
+        edge(n + sx, cmul(fyz, op.Q[0][p.i]),
+             ADJ && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.j > 0)
+        edge(n - sy, cmul(fxz, op.Q[1][p.j - 1]),
+             ADJ && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
+    if (p.j < op.ny - 1)
+        edge(n + sy, cmul(fxz, op.Q[1][p.j]),
+             ADJ && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
+    if (p.k > 0)
+        edge(n - sz, cmul(fxy, op.Q[2][p.k - 1]),
+             ADJ && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
+    if (p.k < op.nz - 1)
+        edge(n + sz, cmul(fxy, op.Q[2][p.k]),
+             ADJ && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
+    return cadd(un, cscale(acc, me.y));
+}
+
+// Row of the unscaled fp64 operator at node n applied to x (complex128).
+//   A     : fixed -> x_n ; else A_nn x_n + sum_j e_nj x_j
+//   A^H   : conj(A_nn) x_n + sum_{j not fixed} conj(e_nj) x_j
+//   |A|   : fixed -> |x_n| ; else |A_nn||x_n| + sum_j |e_nj||x_j|
+//   |A^H| : |A_nn||x_n| + sum_{j not fixed} |e_nj||x_j|
+template <int VARIANT>
+__device__ __forceinline__ double2 a_row(const OpView<double>& op,
+                                         const double2* __restrict__ x, long long n, Node p) {
+    constexpr bool H = (VARIANT == USV_APPLY_AH || VARIANT == USV_APPLY_ABS_AH);
+    constexpr bool ABS = (VARIANT == USV_APPLY_ABS_A || VARIANT == USV_APPLY_ABS_AH);
+    const double2 xn = x[n];
+    const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
+    if (!H && fixed) return ABS ? make_double2(cabs(xn), 0.0) : xn;
+    const double rho = op.rec[n].x;
+    const double2 d = op.d[n];
+    double2 acc = ABS ? make_double2(cabs(d) * cabs(xn), 0.0) : (H ? cmulc(d, xn) : cmul(d, xn));
+    const double2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
+    const double2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
+    auto edge = [&](long long m, double2 F, bool nb_fixed) {
+        if (H && nb_fixed) return;
+        const double g = 2.0 / (rho + op.rec[m].x);
+        const double2 e = cscale(F, g);
+        const double2 xm = x[m];
+        if (ABS) acc.x += cabs(e) * cabs(xm);
+        else acc = cadd(acc, H ? cmulc(e, xm) : cmul(e, xm));
+    };
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+    if (p.i > 0)
+        edge(n - 1, cmul(fyz, op.Q[0][p.i - 1]),
+             H && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.i < op.nx - 1)
+        edge(n + 1, cmul(fyz, op.Q[0][p.i]),
+             H && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.j > 0)
+        edge(n - sy, cmul(fxz, op.Q[1][p.j - 1]),
+             H && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
+    if (p.j < op.ny - 1)
+        edge(n + sy, cmul(fxz, op.Q[1][p.j]),
+             H && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
+    if (p.k > 0)
+        edge(n - sz, cmul(fxy, op.Q[2][p.k - 1]),
+             H && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
+    if (p.k < op.nz - 1)
+        edge(n + sz, cmul(fxy, op.Q[2][p.k]),
+             H && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
+    return acc;
+}
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Sum over the block (blockDim.x a multiple of 32, <= 1024); result valid in
+// every thread. `sh` needs 32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double t = (lane < nw) ? sh[lane] : 0.0;
+    return warp_sum(t);
+}
+__device__ __forceinline__ double block_max(double v, double* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_max(v);
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double t = (lane < nw) ? sh[lane] : 0.0;
+    return warp_max(t);
+}
+
+// Status helpers shared by the translation units.
+int set_last_cuda_error(cudaError_t e);
+}  // namespace usv
+
+#define USV_CUDA_TRY(expr)                                              \
+    do {                                                                \
+        cudaError_t _e = (expr);                                        \
+        if (_e != cudaSuccess) return ::usv::set_last_cuda_error(_e);   \
+    } while (0)

@@ -1,0 +1,130 @@
+"""Row-scaled Jacobi GMRES on the B200: the drop-in for GpuIterativeSolver.
+
+Mirrors src/algorithm/solvers/iterative_solver.py:12-104 — same constructor
+arguments and defaults, same stats attributes (last_iterations,
+last_scaled_residual, last_backward_error), same acceptance gates and the
+same RuntimeError message — but the operator is the matrix-free sm_100a
+stencil and the whole restarted GMRES runs in CUDA (usv_gmres_solve),
+batched over right-hand sides.
+
+precision="mixed": complex64 Krylov vectors and stencil inside each cycle,
+FP64 Gram-Schmidt dots, Hessenberg/Givens, true residual and solution update
+(iterative refinement at every restart). precision="fp64": complex128
+throughout — the plain FP64 comparator.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _native as N
+
+_PRECISIONS = {"mixed": N.PREC_MIXED, "fp64": N.PREC_FP64, "complex64": N.PREC_MIXED,
+               "complex128": N.PREC_FP64}
+
+
+class B200IterativeSolver:
+    """GPU row-scaled Jacobi-GMRES solver for the matrix-free Helmholtz operator."""
+
+    def __init__(self, restart: int = 30, maxiter: int = 3000, rtol: float = 1.0e-6,
+                 backward_error_tol: float = 1.0e-4, precision: str = "mixed",
+                 full_cycles: bool = True, use_graph: bool = True, block_nodes: int = 0,
+                 verbose: bool = False, profile: bool = False):
+        if str(precision).lower() not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        self.restart = int(restart)
+        self.maxiter = int(maxiter)
+        self.rtol = float(rtol)
+        self.backward_error_tol = float(backward_error_tol)
+        self.precision = str(precision).lower()
+        self.full_cycles = bool(full_cycles)
+        self.use_graph = bool(use_graph)
+        self.block_nodes = int(block_nodes)
+        self.verbose = bool(verbose)
+        self.profile = bool(profile)
+        self.last_profile = None
+        self.last_iterations = 0
+        self.last_scaled_residual = None
+        self.last_backward_error = None
+        self.last_stats = []
+        self.last_history = []
+
+    def history_capacity(self) -> int:
+        return self.maxiter // max(self.restart, 1) + 2
+
+    def params(self, adjoint: bool = False) -> N.GmresParams:
+        p = N.GmresParams()
+        p.restart, p.maxiter = self.restart, self.maxiter
+        p.rtol, p.backward_error_tol = self.rtol, self.backward_error_tol
+        p.precision = _PRECISIONS[self.precision]
+        p.adjoint = 1 if adjoint else 0
+        p.full_cycles = 1 if self.full_cycles else 0
+        p.use_graph = 1 if self.use_graph else 0
+        p.block_nodes = self.block_nodes
+        p.history_capacity = self.history_capacity()
+        return p
+
+    def workspace_bytes(self, operator, nrhs: int, adjoint: bool = False) -> int:
+        nbytes = C.c_size_t()
+        p = self.params(adjoint)
+        N.check(N.load().usv_gmres_workspace_bytes(C.byref(operator.scene), C.byref(p), int(nrhs),
+                                                   C.byref(nbytes)), "gmres workspace")
+        return nbytes.value
+
+    def solve(self, operator, rhs: torch.Tensor, adjoint: bool = False,
+              raise_on_failure: bool = True) -> torch.Tensor:
+        """Solve A x = rhs (or A^H x = rhs) on the device.
+
+        rhs: complex128 device tensor of shape (N,) or (B, N) (row b is one
+        right-hand side). Returns x with the same shape.
+        """
+        squeeze = rhs.dim() == 1
+        b = rhs.reshape(1, -1) if squeeze else rhs
+        if b.shape[-1] != operator.n:
+            raise ValueError("rhs length does not match the operator")
+        b = b.to(device=operator.device, dtype=torch.complex128).contiguous()
+        nrhs = b.shape[0]
+        x = torch.empty_like(b)
+        p = self.params(adjoint)
+        nbytes = self.workspace_bytes(operator, nrhs, adjoint)
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=operator.device)
+        stats = (N.GmresStats * nrhs)()
+        hcap = p.history_capacity
+        hist = (C.c_double * (hcap * nrhs))()
+        p.history = C.cast(hist, C.POINTER(C.c_double))
+        prof = N.GmresProfile() if self.profile else None
+        if prof is not None:
+            p.profile = C.pointer(prof)
+        with torch.cuda.device(operator.device):
+            N.check(N.load().usv_gmres_solve(C.byref(operator.scene), N.ptr(operator.buffer),
+                                             C.byref(p), N.ptr(b), N.ptr(x), nrhs, operator.n,
+                                             N.ptr(ws), nbytes, stats,
+                                             N.stream_handle(torch, operator.device)),
+                    "gmres")
+        del ws
+        self.last_stats = [dict(status=s.status, info=s.info, iterations=s.iterations,
+                                cycles=s.cycles, scaled_residual=s.scaled_residual,
+                                backward_error=s.backward_error,
+                                initial_residual=s.initial_residual) for s in stats]
+        self.last_history = [list(hist[k * hcap:k * hcap + min(s.cycles, hcap)])
+                             for k, s in enumerate(stats)]
+        if prof is not None:
+            self.last_profile = {name: dict(launches=prof.launches[i], ms=prof.milliseconds[i],
+                                            bytes=prof.bytes[i])
+                                 for i, name in enumerate(N.KFAMILY_NAMES)}
+        self.last_iterations = max(s.iterations for s in stats)
+        self.last_scaled_residual = max(s.scaled_residual for s in stats)
+        self.last_backward_error = max(s.backward_error for s in stats)
+        if raise_on_failure:
+            for s in stats:
+                if s.status != N.USV_OK:
+                    raise RuntimeError(
+                        f"info={s.info}, iterations={s.iterations}, "
+                        f"scaled residual={s.scaled_residual:.3e}, "
+                        f"backward error={s.backward_error:.3e}")
+        if self.verbose:
+            print(f"  --> GMRES iterations: {self.last_iterations} | scaled relative residual: "
+                  f"{self.last_scaled_residual:.3e} | backward error: "
+                  f"{self.last_backward_error:.3e}")
+        return x[0] if squeeze else x
