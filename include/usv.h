@@ -60,6 +60,7 @@ extern "C" {
 #define USV_ERR_SOURCE_PML 6     /* deposited aperture overlaps the PML          */
 #define USV_ERR_SOURCE_SOFT 7    /* deposited aperture touches a soft face       */
 #define USV_ERR_SOURCE_CLEARANCE 8 /* aperture closer than one cell to a side    */
+#define USV_ERR_TOO_LARGE 9      /* size beyond a fixed internal maximum          */
 
 /* face kinds, faces in the reference order -x,+x,-y,+y,-z,+z */
 #define USV_FACE_REFLECTING 0
@@ -204,6 +205,20 @@ int usv_basis_adjoint(const void* basis, int64_t n, int m, int basis_precision,
                       const void* cotangent, const double* phases, double* response,
                       double* grad, void* workspace, size_t workspace_bytes,
                       void* stream);
+/* usv_basis_adjoint without a workspace, for callers that cannot allocate
+ * device memory when they need the gradient (a process whose device memory
+ * is owned by its own pool, a real-time loop that must not pay cudaMalloc
+ * latency or risk out-of-memory, code running during CUDA graph capture).
+ * It has no counterpart in the reference. The partial sums live in a 1 MiB
+ * file-scope device array that every GPU loading this library holds until
+ * exit; m (emitters) is limited to 4096, larger m returns USV_ERR_TOO_LARGE.
+ * The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams or
+ * threads) race and must be serialised by the caller. */
+int usv_basis_adjoint_noalloc(const void* basis, int64_t n, int m, int basis_precision,
+                              const void* cotangent, const double* phases,
+                              double* response, double* grad, void* stream);
 int usv_basis_target_response(const void* basis, int64_t nx, int64_t ny, int64_t nz,
                               int m, int basis_precision, const double* points, int p,
                               double dx, void* out, void* stream);

@@ -21,6 +21,7 @@ USV_ERR_NONFINITE = 5
 USV_ERR_SOURCE_PML = 6
 USV_ERR_SOURCE_SOFT = 7
 USV_ERR_SOURCE_CLEARANCE = 8
+USV_ERR_TOO_LARGE = 9
 
 FACE_REFLECTING, FACE_OPEN, FACE_SOFT, FACE_IMPEDANCE = 0, 1, 2, 3
 APPLY_A, APPLY_AH, APPLY_ABS_A, APPLY_ABS_AH, APPLY_K, APPLY_KH = range(6)
@@ -87,6 +88,7 @@ _SIGNATURES = {
     "usv_basis_field": ([_P, _I64, _I, _I, _P, _P, _P], _I),
     "usv_basis_adjoint_workspace_bytes": ([_I64, _I, C.POINTER(_SZ)], _I),
     "usv_basis_adjoint": ([_P, _I64, _I, _I, _P, _P, _P, _P, _P, _SZ, _P], _I),
+    "usv_basis_adjoint_noalloc": ([_P, _I64, _I, _I, _P, _P, _P, _P, _P], _I),
     "usv_basis_target_response": ([_P, _I64, _I64, _I64, _I, _I, _P, _I, _D, _P, _P], _I),
 }
 
@@ -133,7 +135,7 @@ def check(status: int, what: str = "usv") -> None:
         return
     msg = f"{what}: {status_string(status)}"
     if status in (USV_ERR_ARG, USV_ERR_SOURCE_PML, USV_ERR_SOURCE_SOFT,
-                  USV_ERR_SOURCE_CLEARANCE, USV_ERR_WORKSPACE):
+                  USV_ERR_SOURCE_CLEARANCE, USV_ERR_WORKSPACE, USV_ERR_TOO_LARGE):
         raise ValueError(msg)
     raise RuntimeError(msg)
 

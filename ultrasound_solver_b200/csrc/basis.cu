@@ -183,3 +183,96 @@ int usv_basis_target_response(const void* basis, int64_t nx, int64_t ny, int64_t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// No-allocation variant of usv_basis_adjoint.
+//
+// Some callers cannot allocate device memory when they need the phase
+// gradient: an application that hands all device memory to its own pool at
+// start-up, a real-time control loop that must not pay cudaMalloc latency or
+// risk an out-of-memory failure mid-run, or host code running while a CUDA
+// graph is being captured (where cudaMalloc is not allowed). For them the
+// per-chunk partial sums live in the file-scope array below instead of a
+// caller workspace. It is 1 MiB and every GPU that loads this library keeps it
+// until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace usv {
+
+constexpr long long kNoAllocPartials = 1LL << 16;  // double2 entries = 1 MiB
+constexpr int kNoAllocMaxEmitters = 4096;
+static __device__ __align__(256) double2 g_noalloc_partials[kNoAllocPartials];
+
+// Same partial sums as k_basis_dots, but each CTA walks chunk, chunk+nblk, ...
+// so the partial count nblk*M stays inside the static array for any N.
+template <typename C2>
+__global__ void __launch_bounds__(256) k_basis_dots_strided(const C2* G, long long N, int chunk,
+                                                            const double2* g, double2* partial) {
+    const int m = blockIdx.y;
+    __shared__ double sh[32];
+    const C2* col = G + (long long)m * N;
+    double re = 0.0, im = 0.0;
+    for (long long n0 = (long long)blockIdx.x * chunk; n0 < N; n0 += (long long)gridDim.x * chunk) {
+        const long long n1 = min(n0 + chunk, N);
+        for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+            const double2 a = to_d(col[n]), b = g[n];
+            re = fma(a.x, b.x, fma(a.y, b.y, re));
+            im = fma(a.x, b.y, fma(-a.y, b.x, im));
+        }
+    }
+    re = block_sum(re, sh);
+    im = block_sum(im, sh);
+    if (threadIdx.x == 0) partial[(long long)m * gridDim.x + blockIdx.x] = make_double2(re, im);
+}
+
+// Device address of g_noalloc_partials, resolved once per device.
+static int noalloc_scratch(double2** out) {
+    static std::mutex lock;
+    static void* addr[256] = {};
+    int dev = 0;
+    USV_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return USV_ERR_ARG;
+    std::lock_guard<std::mutex> guard(lock);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        USV_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_partials));
+        addr[dev] = p;
+    }
+    *out = static_cast<double2*>(addr[dev]);
+    return USV_OK;
+}
+
+}  // namespace usv
+
+extern "C" int usv_basis_adjoint_noalloc(const void* basis, int64_t n, int m, int prec,
+                                         const void* cotangent, const double* phases,
+                                         double* response, double* grad, void* stream) {
+    using namespace usv;
+    if (!basis || n < 1 || m < 1 || !cotangent || !phases) return USV_ERR_ARG;
+    if (m > kNoAllocMaxEmitters) return USV_ERR_TOO_LARGE;
+    if (prec != USV_PREC_MIXED && prec != USV_PREC_FP64) return USV_ERR_ARG;
+    double2* part = nullptr;
+    int st = noalloc_scratch(&part);
+    if (st) return st;
+    const long long chunks = (n + kBasisChunk - 1) / kBasisChunk;
+    const long long cap = kNoAllocPartials / m;
+    const int nblk = int(chunks < cap ? chunks : cap);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    dim3 grid(nblk, m);
+    // every partial slot [m][0..nblk) is written before k_basis_finish reads it,
+    // so stale contents of the shared array never reach the result
+    if (prec == USV_PREC_MIXED)
+        k_basis_dots_strided<float2><<<grid, 256, 0, s>>>(static_cast<const float2*>(basis), n,
+                                                          kBasisChunk,
+                                                          static_cast<const double2*>(cotangent), part);
+    else
+        k_basis_dots_strided<double2><<<grid, 256, 0, s>>>(static_cast<const double2*>(basis), n,
+                                                           kBasisChunk,
+                                                           static_cast<const double2*>(cotangent), part);
+    USV_CUDA_TRY(cudaGetLastError());
+    k_basis_finish<<<m, 256, 0, s>>>(part, nblk, m, phases, reinterpret_cast<double2*>(response),
+                                     grad);
+    USV_CUDA_TRY(cudaGetLastError());
+    return USV_OK;
+}

@@ -250,6 +250,8 @@ const char* usv_status_string(int status) {
         case USV_ERR_SOURCE_SOFT: return "Sinc flux conflicts with a pressure-release boundary";
         case USV_ERR_SOURCE_CLEARANCE:
             return "Sinc aperture needs one grid cell clearance from side boundaries";
+        case USV_ERR_TOO_LARGE:
+            return "size exceeds the fixed maximum of the no-allocation entry point";
         default: return "unknown status";
     }
 }
