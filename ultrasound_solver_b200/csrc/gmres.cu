@@ -115,7 +115,7 @@ __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
 template <bool ADJ, typename C2>
 __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const double2* rhs,
                                                   const double2* x, long long ld, C2* V,
-                                                  GState g, int first) {
+                                                  GState g, int first, Step step) {
     const int b = blockIdx.y;
     if (!first && (g.status[b] != ST_ACTIVE)) return;
     __shared__ double sh[32];
@@ -125,13 +125,14 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
     const double2* xb = x + b * ld;
     C2* v0 = V + (long long)b * (g.m + 1) * g.nv;
     double acc = 0.0;
+    Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
     for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
         double2 r = rb[n];
         if (!first) {
-            const double2 ax = a_row<ADJ ? USV_APPLY_AH : USV_APPLY_A>(op, xb, n,
-                                                                       decode(n, op.nx, op.ny));
+            const double2 ax = a_row<ADJ ? USV_APPLY_AH : USV_APPLY_A>(op, xb, n, p);
             r = csub(r, ax);
         }
+        advance(p, step, op.nx, op.ny);
         r = cscale(r, op.rec[n].y);
         const C2 rv = from_d<C2>(r);
         v0[n] = rv;
@@ -176,44 +177,75 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
 
 // ------------------------------------------------------------ Arnoldi: stencil + dots
 // A CTA owns a chunk of kChunk consecutive nodes. Streaming passes over the
-// Krylov basis work on node PAIRS: thread t loads the 16-byte (complex64) or
-// 2x16-byte (complex128) pair at 2t + 2*kThreads*k, so a warp reads 512 B
-// contiguous per vector and each thread keeps kPairs x kTU loads in flight.
+// Krylov basis work on node PAIRS: thread t owns the pairs at node offsets
+// 2(t + kThreads k), k < kPairs, so a warp touches 512 B (complex64) or 1 KB
+// (complex128) contiguous per vector. Basis vectors reach shared memory
+// through a per-thread cp.async pipeline of kStages(R) stages: each thread
+// copies, waits for and reads only its own 16-byte slots, so the pipeline
+// needs no CTA barrier and holds no loads in registers.
 constexpr int kThreads = 256;
 constexpr int kPairs = 4;
-constexpr int kTU = 2;
+constexpr int kTU = 8;                          // basis vectors per CTA reduction
 constexpr int kChunk = 2 * kThreads * kPairs;  // 2048 nodes
 
-__device__ __forceinline__ void ld_pair(const float2* p, double2& a, double2& b) {
-    const float4 v = __ldcs(reinterpret_cast<const float4*>(p));
-    a = make_double2(v.x, v.y);
-    b = make_double2(v.z, v.w);
-}
-__device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b) {
-    a = __ldcs(p);
-    b = __ldcs(p + 1);
-}
-// Raw pair kept in registers in the vector precision until it is used.
-template <typename C2> struct RawPair;
-template <> struct RawPair<float2> {
-    float4 v;
-    __device__ __forceinline__ void load(const float2* p) {
-        v = __ldcs(reinterpret_cast<const float4*>(p));
-    }
-    __device__ __forceinline__ void zero() { v = make_float4(0.f, 0.f, 0.f, 0.f); }
-    __device__ __forceinline__ double2 get(int c) const {
-        return c ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
-    }
+template <typename C2> struct Pipe {
+    static constexpr int UPP = int(sizeof(C2) / 8);            // 16-B units per pair: 1 or 2
+    static constexpr int S = UPP == 1 ? 4 : 3;                  // stages
+    static constexpr int STAGE_UNITS = kPairs * UPP * kThreads;
+    static constexpr size_t BYTES = size_t(S) * STAGE_UNITS * 16;
 };
-template <> struct RawPair<double2> {
-    double2 a, b;
-    __device__ __forceinline__ void load(const double2* p) {
-        a = __ldcs(p);
-        b = __ldcs(p + 1);
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Stage basis vector t (chunk at `base`, `len` valid nodes) into stage t % S;
+// slots of pairs outside the chunk (or t > last) are zero-filled, no read.
+template <typename C2>
+__device__ __forceinline__ void stage_vector(uint4* stg, const C2* base, int t, int last,
+                                             int len) {
+    using P = Pipe<C2>;
+    const int s = t % P::S;
+    const char* src0 = reinterpret_cast<const char*>(base);
+#pragma unroll
+    for (int k = 0; k < kPairs; ++k) {
+        const int e = 2 * (threadIdx.x + k * kThreads);
+        const bool ok = t <= last && e < len;
+#pragma unroll
+        for (int h = 0; h < P::UPP; ++h) {
+            uint4* dst = stg + ((s * kPairs + k) * P::UPP + h) * kThreads + threadIdx.x;
+            const char* src = ok ? src0 + size_t(e) * sizeof(C2) + 16 * h : src0;
+            cp_async16(dst, src, ok ? 16 : 0);
+        }
     }
-    __device__ __forceinline__ void zero() { a = b = make_double2(0.0, 0.0); }
-    __device__ __forceinline__ double2 get(int c) const { return c ? b : a; }
-};
+    cp_async_commit();
+}
+
+// Complex value c (0/1) of pair k of stage t % S, widened to double.
+template <typename C2>
+__device__ __forceinline__ double2 staged(const uint4* stg, int t, int k, int c);
+template <>
+__device__ __forceinline__ double2 staged<float2>(const uint4* stg, int t, int k, int c) {
+    const int s = t % Pipe<float2>::S;
+    const float4 v = reinterpret_cast<const float4*>(stg)[(s * kPairs + k) * kThreads + threadIdx.x];
+    return c ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
+}
+template <>
+__device__ __forceinline__ double2 staged<double2>(const uint4* stg, int t, int k, int c) {
+    const int s = t % Pipe<double2>::S;
+    return reinterpret_cast<const double2*>(stg)[((s * kPairs + k) * 2 + c) * kThreads + threadIdx.x];
+}
+
 __device__ __forceinline__ void st_pair(float2* p, double2 a, double2 b) {
     *reinterpret_cast<float4*>(p) = make_float4(float(a.x), float(a.y), float(b.x), float(b.y));
 }
@@ -221,20 +253,87 @@ __device__ __forceinline__ void st_pair(double2* p, double2 a, double2 b) {
     p[0] = a;
     p[1] = b;
 }
+__device__ __forceinline__ void ld_pair(const float2* p, double2& a, double2& b) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a = make_double2(v.x, v.y);
+    b = make_double2(v.z, v.w);
+}
+__device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b) {
+    a = p[0];
+    b = p[1];
+}
 // value actually stored (rounded to the vector precision)
 __device__ __forceinline__ double2 rounded(const float2*, double2 a) {
     return make_double2(double(float(a.x)), double(float(a.y)));
 }
 __device__ __forceinline__ double2 rounded(const double2*, double2 a) { return a; }
 
+// Stream basis vectors t = first..last (t relative to `base`, stride nv) and
+// call f(t, k, c, value) for every pair slot of this thread. complex64 goes
+// through the cp.async pipeline (the caller has already issued the first
+// kStages-1 vectors when `prefetched`); complex128 uses direct 16-byte loads
+// unrolled over kUnroll vectors, which keeps enough bytes in flight with the
+// wider elements.
+constexpr int kUnroll = 2;
+template <typename C2, typename F>
+__device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long long nv, int last,
+                                             int len, bool prefetched, F&& f) {
+    if constexpr (Pipe<C2>::UPP == 1) {
+        using P = Pipe<C2>;
+        auto issue = [&](int t) {
+            stage_vector<C2>(stg, base + (long long)(t <= last ? t : 0) * nv, t, last, len);
+        };
+        if (!prefetched) {
+#pragma unroll
+            for (int t = 0; t < P::S - 1; ++t) issue(t);
+        }
+        for (int t = 0; t <= last; ++t) {
+            issue(t + P::S - 1);
+            cp_async_wait<P::S - 1>();
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) f(t, k, c, staged<C2>(stg, t, k, c));
+        }
+        cp_async_wait<0>();
+    } else {
+        for (int t0 = 0; t0 <= last; t0 += kUnroll) {
+            double2 v[kUnroll][kPairs][2];
+#pragma unroll
+            for (int q = 0; q < kUnroll; ++q)
+#pragma unroll
+                for (int k = 0; k < kPairs; ++k) {
+                    const int e = 2 * (threadIdx.x + k * kThreads);
+                    if (t0 + q <= last && e < len)
+                        ld_pair(base + (long long)(t0 + q) * nv + e, v[q][k][0], v[q][k][1]);
+                    else
+                        v[q][k][0] = v[q][k][1] = make_double2(0.0, 0.0);
+                }
+#pragma unroll
+            for (int q = 0; q < kUnroll; ++q)
+                if (t0 + q <= last) {
+#pragma unroll
+                    for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                        for (int c = 0; c < 2; ++c) f(t0 + q, k, c, v[q][k][c]);
+                }
+        }
+    }
+}
+
+// Dots of w with u_0..u_j: one warp per (basis vector, segment of the chunk),
+// lanes over 16-byte pairs with kDotUnroll loads in flight, one warp reduction
+// per task; segments per vector grow when j is small so all warps work.
+constexpr int kDotUnroll = 8;
+
 template <typename R, bool ADJ>
 __global__ void __launch_bounds__(kThreads) k_dots(OpView<R> op, typename Tr<R>::c2* V, GState g,
-                                                   int j) {
+                                                   int j, Step step) {
     using C2 = typename Tr<R>::c2;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
     __shared__ __align__(16) C2 ys[kChunk];
-    __shared__ double2 red[kThreads / 32][kTU];
+    __shared__ double2 segsum[USV_MAX_RESTART + 2][kThreads / 32];
     const long long N = op.n;
     const long long n0 = (long long)blockIdx.x * kChunk;
     const int len = int(min((long long)kChunk, N - n0));
@@ -242,82 +341,75 @@ __global__ void __launch_bounds__(kThreads) k_dots(OpView<R> op, typename Tr<R>:
     const C2* uj = Vb + (long long)j * g.nv;
     C2* w = Vb + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
+    Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
 #pragma unroll 2
     for (int e = threadIdx.x; e < kChunk; e += kThreads) {
         C2 y = cmake<C2>(0.0, 0.0);
         if (e < len) {
             const long long n = n0 + e;
-            y = cscale(k_row<R, ADJ>(op, uj, n, decode(n, op.nx, op.ny)), sj);
+            y = cscale(k_row<R, ADJ>(op, uj, n, p), sj);
             w[n] = y;
         }
         ys[e] = y;
+        advance(p, step, op.nx, op.ny);
     }
     __syncthreads();
-    // dots with u_0..u_j over the chunk: every thread owns kPairs pairs;
-    // tiles of kTU basis vectors are reduced across the CTA through `red`.
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double2 yv[kPairs][2];
+    constexpr int nw = kThreads / 32;
+    const int tasks_t = j + 2;  // t = 0..j dots, t = j+1: ||w||^2
+    int segs = 1;
+    while (segs < nw && tasks_t * segs < nw) segs <<= 1;
+    const int npairs = (len + 1) / 2;
+    const int per_seg = (npairs + segs - 1) / segs;
+    for (int task = warp; task < tasks_t * segs; task += nw) {
+        const int t = task / segs, seg = task % segs;
+        const int q0 = seg * per_seg, q1 = min(npairs, q0 + per_seg);
+        double re = 0.0, im = 0.0;
+        if (t <= j) {
+            const C2* ut = Vb + (long long)t * g.nv + n0;
+            for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
+                double2 a[kDotUnroll][2];
 #pragma unroll
-    for (int k = 0; k < kPairs; ++k) {
-        const int e = 2 * (threadIdx.x + k * kThreads);
-        yv[k][0] = to_d(ys[e]);
-        yv[k][1] = to_d(ys[e + 1]);
-    }
-    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * (g.m + 2);
-    for (int t0 = 0; t0 <= j; t0 += kTU) {
-        double2 acc[kTU];
+                for (int u = 0; u < kDotUnroll; ++u) {
+                    const int q = qb + 32 * u;
+                    if (q < q1) ld_pair(ut + 2 * q, a[u][0], a[u][1]);
+                    else a[u][0] = a[u][1] = make_double2(0.0, 0.0);
+                }
 #pragma unroll
-        for (int q = 0; q < kTU; ++q) acc[q] = make_double2(0.0, 0.0);
+                for (int u = 0; u < kDotUnroll; ++u) {
+                    const int q = min(qb + 32 * u, npairs - 1);
 #pragma unroll
-        for (int q = 0; q < kTU; ++q) {
-            const int t = t0 + q;
-            if (t <= j) {
-                const C2* ut = Vb + (long long)t * g.nv + n0;
-#pragma unroll
-                for (int k = 0; k < kPairs; ++k) {
-                    const int e = 2 * (threadIdx.x + k * kThreads);
-                    if (e < len) {
-                        RawPair<C2> rp;
-                        rp.load(ut + e);
-                        const double2 a0 = rp.get(0), a1 = rp.get(1);
-                        acc[q].x += a0.x * yv[k][0].x + a0.y * yv[k][0].y
-                                  + a1.x * yv[k][1].x + a1.y * yv[k][1].y;
-                        acc[q].y += a0.x * yv[k][0].y - a0.y * yv[k][0].x
-                                  + a1.x * yv[k][1].y - a1.y * yv[k][1].x;
+                    for (int c = 0; c < 2; ++c) {
+                        const double2 y = to_d(ys[2 * q + c]);
+                        re = fma(a[u][c].x, y.x, fma(a[u][c].y, y.y, re));
+                        im = fma(a[u][c].x, y.y, fma(-a[u][c].y, y.x, im));
                     }
                 }
             }
+        } else {
+            for (int q = q0 + lane; q < q1; q += 32)
+                re += cabs2(to_d(ys[2 * q])) + cabs2(to_d(ys[2 * q + 1]));
         }
-#pragma unroll
-        for (int q = 0; q < kTU; ++q) {
-            acc[q].x = warp_sum(acc[q].x);
-            acc[q].y = warp_sum(acc[q].y);
-        }
-        __syncthreads();
-        if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < kTU; ++q) red[warp][q] = acc[q];
-        }
-        __syncthreads();
-        if (threadIdx.x < kTU && t0 + threadIdx.x <= j) {
-            double re = 0.0, im = 0.0;
-            for (int wv = 0; wv < kThreads / 32; ++wv) {
-                re += red[wv][threadIdx.x].x;
-                im += red[wv][threadIdx.x].y;
-            }
-            const double st = g.sigma[b * (g.m + 1) + t0 + threadIdx.x];
-            part[t0 + threadIdx.x] = make_double2(re * st, im * st);
-        }
+        re = warp_sum(re);
+        im = warp_sum(im);
+        if (lane == 0) segsum[t][seg] = make_double2(re, im);
     }
-    // ||w||^2 (breakdown reference)
-    double nw2 = 0.0;
-#pragma unroll
-    for (int k = 0; k < kPairs; ++k) nw2 += cabs2(yv[k][0]) + cabs2(yv[k][1]);
-    __shared__ double sh[32];
-    nw2 = block_sum(nw2, sh);
-    if (threadIdx.x == 0) part[j + 1] = make_double2(nw2, 0.0);
+    __syncthreads();
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * (g.m + 2);
+    for (int t = threadIdx.x; t < tasks_t; t += kThreads) {
+        double re = 0.0, im = 0.0;
+        for (int sg = 0; sg < segs; ++sg) {
+            re += segsum[t][sg].x;
+            im += segsum[t][sg].y;
+        }
+        if (t <= j) {
+            const double st = g.sigma[b * (g.m + 1) + t];
+            re *= st;
+            im *= st;
+        }
+        part[t] = make_double2(re, im);
+    }
     if (!last_block_done(&g.counter[b], g.nblk)) return;
-    const int nw = kThreads >> 5;
     for (int t = warp; t <= j + 1; t += nw) {
         double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
         const double2* pt = g.partial + (long long)b * g.nblk * (g.m + 2) + t;
@@ -356,11 +448,13 @@ __device__ __forceinline__ double reduce_slot0(const GState& g, int b, double* s
 
 // ------------------------------------------------------------ Arnoldi: orthogonalise + norm
 template <typename R>
-__global__ void __launch_bounds__(kThreads, 2) k_orth(typename Tr<R>::c2* V, long long N, GState g,
+__global__ void __launch_bounds__(kThreads) k_orth(typename Tr<R>::c2* V, long long N, GState g,
                                                    int j) {
     using C2 = typename Tr<R>::c2;
+    using P = Pipe<C2>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    extern __shared__ __align__(16) uint4 stg[];
     __shared__ double2 hs[USV_MAX_RESTART + 2];
     __shared__ double2 gsS[USV_MAX_RESTART + 1];
     __shared__ double gcS[USV_MAX_RESTART + 1];
@@ -368,11 +462,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_orth(typename Tr<R>::c2* V, lon
     const int m = g.m;
     for (int t = threadIdx.x; t <= j; t += kThreads)
         hs[t] = cscale(g.H[((long long)b * m + j) * (m + 1) + t], g.sigma[b * (m + 1) + t]);
-    __syncthreads();
     const long long n0 = (long long)blockIdx.x * kChunk;
     const int len = int(min((long long)kChunk, N - n0));
     C2* Vb = V + (long long)b * (m + 1) * g.nv;
     C2* w = Vb + (long long)(j + 1) * g.nv + n0;
+    const C2* base = Vb + n0;
     double2 u[kPairs][2];
 #pragma unroll
     for (int k = 0; k < kPairs; ++k) {
@@ -380,31 +474,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_orth(typename Tr<R>::c2* V, lon
         if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
         else u[k][0] = u[k][1] = make_double2(0.0, 0.0);
     }
-    for (int t0 = 0; t0 <= j; t0 += kTU) {
-        RawPair<C2> v[kTU][kPairs];
-#pragma unroll
-        for (int q = 0; q < kTU; ++q) {
-            const C2* vt = Vb + (long long)(t0 + q) * g.nv + n0;
-#pragma unroll
-            for (int k = 0; k < kPairs; ++k) {
-                const int e = 2 * (threadIdx.x + k * kThreads);
-                if (t0 + q <= j && e < len) v[q][k].load(vt + e);
-                else v[q][k].zero();
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kTU; ++q) {
-            const double2 h = (t0 + q <= j) ? hs[t0 + q] : make_double2(0.0, 0.0);
-#pragma unroll
-            for (int k = 0; k < kPairs; ++k)
-#pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const double2 vv = v[q][k].get(c);
-                    u[k][c].x -= h.x * vv.x - h.y * vv.y;
-                    u[k][c].y -= h.x * vv.y + h.y * vv.x;
-                }
-        }
-    }
+    __syncthreads();  // hs visible
+    stream_basis<C2>(stg, base, g.nv, j, len, false, [&](int t, int k, int c, double2 vv) {
+        const double2 h = hs[t];
+        u[k][c].x -= h.x * vv.x - h.y * vv.y;
+        u[k][c].y -= h.x * vv.y + h.y * vv.x;
+    });
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < kPairs; ++k) {
@@ -514,43 +589,28 @@ __global__ void __launch_bounds__(128) k_lsq(GState g) {
 
 // ------------------------------------------------------------ solution update (fp64)
 template <typename R>
-__global__ void __launch_bounds__(kThreads, 2) k_update(OpView<double> op,
+__global__ void __launch_bounds__(kThreads) k_update(OpView<double> op,
                                                      const typename Tr<R>::c2* V, double2* x,
                                                      long long ld, GState g) {
     using C2 = typename Tr<R>::c2;
+    using P = Pipe<C2>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
-    __shared__ double2 ys[USV_MAX_RESTART + kTU];
+    extern __shared__ __align__(16) uint4 stg[];
+    __shared__ double2 ys[USV_MAX_RESTART];
     const int L = g.len[b];
-    for (int t = threadIdx.x; t < L + kTU; t += kThreads)
-        ys[t] = t < L ? g.y[(long long)b * g.m + t] : make_double2(0.0, 0.0);
-    __syncthreads();
+    for (int t = threadIdx.x; t < L; t += kThreads) ys[t] = g.y[(long long)b * g.m + t];
     const long long N = op.n;
     const long long n0 = (long long)blockIdx.x * kChunk;
     const int len = int(min((long long)kChunk, N - n0));
-    const C2* Vb = V + (long long)b * (g.m + 1) * g.nv + n0;
+    const C2* base = V + (long long)b * (g.m + 1) * g.nv + n0;
+    __syncthreads();  // ys visible
     double2 acc[kPairs][2];
 #pragma unroll
     for (int k = 0; k < kPairs; ++k) acc[k][0] = acc[k][1] = make_double2(0.0, 0.0);
-    for (int t0 = 0; t0 < L; t0 += kTU) {
-        RawPair<C2> v[kTU][kPairs];
-#pragma unroll
-        for (int q = 0; q < kTU; ++q)
-#pragma unroll
-            for (int k = 0; k < kPairs; ++k) {
-                const int e = 2 * (threadIdx.x + k * kThreads);
-                if (t0 + q < L && e < len) v[q][k].load(Vb + (long long)(t0 + q) * g.nv + e);
-                else v[q][k].zero();
-            }
-#pragma unroll
-        for (int q = 0; q < kTU; ++q) {
-            const double2 yt = ys[t0 + q];
-#pragma unroll
-            for (int k = 0; k < kPairs; ++k)
-#pragma unroll
-                for (int c = 0; c < 2; ++c) acc[k][c] = cadd(acc[k][c], cmul(yt, v[q][k].get(c)));
-        }
-    }
+    stream_basis<C2>(stg, base, g.nv, L - 1, len, false, [&](int t, int k, int c, double2 vv) {
+        acc[k][c] = cadd(acc[k][c], cmul(ys[t], vv));
+    });
     double2* xb = x + b * ld + n0;
 #pragma unroll
     for (int k = 0; k < kPairs; ++k)
@@ -647,13 +707,24 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     C2* V = reinterpret_cast<C2*>(ws + L.V);
     const dim3 grid(g.nblk, B);
     const size_t lsq_smem = sizeof(double2) * size_t(g.m) * (g.m + 1);
+    const size_t pipe_smem = Pipe<C2>::UPP == 1 ? Pipe<C2>::BYTES : 16;
+    const Step step = make_step(kThreads, s.nx, s.ny);
+    USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(pipe_smem)));
+    USV_CUDA_TRY(cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(pipe_smem)));
     if (lsq_smem > 48 * 1024)
         USV_CUDA_TRY(cudaFuncSetAttribute(k_lsq, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(lsq_smem)));
     // zero the state and the solution
     USV_CUDA_TRY(cudaMemsetAsync(ws + L.state_begin, 0, L.total - L.state_begin, strm));
+    // paired loads may touch the padding past node n-1 of each basis vector:
+    // keep it zero so it contributes nothing to the dots
+    if (g.nv > g.n)
+        USV_CUDA_TRY(cudaMemset2DAsync(V + g.n, g.nv * sizeof(C2), 0, (g.nv - g.n) * sizeof(C2),
+                                       size_t(g.m + 1) * B, strm));
     USV_CUDA_TRY(cudaMemset2DAsync(x, ld * sizeof(double2), 0, g.n * sizeof(double2), B, strm));
-    k_residual<ADJ, C2><<<grid, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1);
+    k_residual<ADJ, C2><<<grid, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
     USV_CUDA_TRY(cudaGetLastError());
 
     // Event timing: one event before the first kernel of a cycle and one after
@@ -679,12 +750,12 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         fam_bytes.clear();
         USV_CUDA_TRY(mark(st, k++, capturing));
         for (int j = 0; j < g.m; ++j) {
-            k_dots<R, ADJ><<<grid, kThreads, 0, st>>>(opk, V, g, j);
+            k_dots<R, ADJ><<<grid, kThreads, 0, st>>>(opk, V, g, j, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
             // read u_0..u_j (u_j also feeds the stencil) + node record, write w
             fam_bytes.push_back(nn * (vb * (j + 2) + 4.0 * sizeof(R)));
-            k_orth<R><<<grid, kThreads, 0, st>>>(V, g.n, g, j);
+            k_orth<R><<<grid, kThreads, pipe_smem, st>>>(V, g.n, g, j);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(1);
             fam_bytes.push_back(nn * vb * (j + 3));
@@ -693,11 +764,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(2);
         fam_bytes.push_back(0.0);
-        k_update<R><<<grid, kThreads, 0, st>>>(op64, V, x, ld, g);
+        k_update<R><<<grid, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(3);
         fam_bytes.push_back(nn * (vb * g.m + 2 * sizeof(double2) + sizeof(double4)));
-        k_residual<ADJ, C2><<<grid, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0);
+        k_residual<ADJ, C2><<<grid, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(4);
         fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));

@@ -196,25 +196,29 @@ static unsigned grid_for(long long n, int threads = 256) {
 // ------------------------------------------------------------ apply kernels
 template <int VARIANT>
 __global__ void __launch_bounds__(256) k_apply_fp64(OpView<double> op, const double2* x,
-                                                    double2* y, long long ld) {
+                                                    double2* y, long long ld, Step step) {
     const int b = blockIdx.y;
     const double2* xb = x + b * ld;
     double2* yb = y + b * ld;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
-         n += (long long)gridDim.x * blockDim.x) {
-        yb[n] = a_row<VARIANT>(op, xb, n, decode(n, op.nx, op.ny));
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    Node p = decode(n, op.nx, op.ny);
+    for (; n < op.n; n += (long long)gridDim.x * blockDim.x) {
+        yb[n] = a_row<VARIANT>(op, xb, n, p);
+        advance(p, step, op.nx, op.ny);
     }
 }
 
 template <typename R, bool ADJ>
 __global__ void __launch_bounds__(256) k_apply_k(OpView<R> op, const typename Tr<R>::c2* x,
-                                                 typename Tr<R>::c2* y, long long ld) {
+                                                 typename Tr<R>::c2* y, long long ld, Step step) {
     const int b = blockIdx.y;
     const auto* xb = x + b * ld;
     auto* yb = y + b * ld;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
-         n += (long long)gridDim.x * blockDim.x) {
-        yb[n] = k_row<R, ADJ>(op, xb, n, decode(n, op.nx, op.ny));
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    Node p = decode(n, op.nx, op.ny);
+    for (; n < op.n; n += (long long)gridDim.x * blockDim.x) {
+        yb[n] = k_row<R, ADJ>(op, xb, n, p);
+        advance(p, step, op.nx, op.ny);
     }
 }
 
@@ -339,34 +343,35 @@ int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant, 
     if (ld < n) return USV_ERR_ARG;
     cudaStream_t strm = static_cast<cudaStream_t>(stream);
     dim3 grid(grid_for(n), nrhs);
+    const Step step = make_step((long long)grid.x * 256, s.nx, s.ny);
     switch (variant) {
         case USV_APPLY_A:
             k_apply_fp64<USV_APPLY_A><<<grid, 256, 0, strm>>>(
-                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld, step);
             break;
         case USV_APPLY_AH:
             k_apply_fp64<USV_APPLY_AH><<<grid, 256, 0, strm>>>(
-                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld, step);
             break;
         case USV_APPLY_ABS_A:
             k_apply_fp64<USV_APPLY_ABS_A><<<grid, 256, 0, strm>>>(
-                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld, step);
             break;
         case USV_APPLY_ABS_AH:
             k_apply_fp64<USV_APPLY_ABS_AH><<<grid, 256, 0, strm>>>(
-                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld);
+                make_view<double>(s, op_buf, false), (const double2*)x, (double2*)y, ld, step);
             break;
         case USV_APPLY_K:
         case USV_APPLY_KH: {
             const bool adj = variant == USV_APPLY_KH;
             if (precision == USV_PREC_FP64) {
                 auto v = make_view<double>(s, op_buf, adj);
-                if (adj) k_apply_k<double, true><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld);
-                else k_apply_k<double, false><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld);
+                if (adj) k_apply_k<double, true><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, step);
+                else k_apply_k<double, false><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, step);
             } else if (precision == USV_PREC_MIXED) {
                 auto v = make_view<float>(s, op_buf, adj);
-                if (adj) k_apply_k<float, true><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld);
-                else k_apply_k<float, false><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld);
+                if (adj) k_apply_k<float, true><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, step);
+                else k_apply_k<float, false><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, step);
             } else {
                 return USV_ERR_ARG;
             }

@@ -161,6 +161,32 @@ struct Node {
     int i, j, k;
 };
 
+// Node-index increment of a fixed flat stride, decomposed once on the host so
+// kernels walk their nodes without integer division.
+struct Step {
+    int di, dj, dk;
+};
+inline Step make_step(long long stride, int nx, int ny) {
+    Step s;
+    s.di = int(stride % nx);
+    s.dj = int((stride / nx) % ny);
+    s.dk = int(stride / ((long long)nx * ny));
+    return s;
+}
+__device__ __forceinline__ void advance(Node& p, const Step& s, int nx, int ny) {
+    p.i += s.di;
+    if (p.i >= nx) {
+        p.i -= nx;
+        p.j += 1;
+    }
+    p.j += s.dj;
+    if (p.j >= ny) {
+        p.j -= ny;
+        p.k += 1;
+    }
+    p.k += s.dk;
+}
+
 __device__ __forceinline__ Node decode(long long n, int nx, int ny) {
     long long t = n / nx;
     Node p;
@@ -168,6 +194,16 @@ __device__ __forceinline__ Node decode(long long n, int nx, int ny) {
     p.k = int(t / ny);
     p.j = int(t - (long long)p.k * ny);
     return p;
+}
+
+// 2 / (a + b): correctly rounded in fp64, fast reciprocal in the complex64
+// inner operator (whose rounding the FP64 restart residual corrects).
+template <typename R> __device__ __forceinline__ R harmonic2(R a, R b);
+template <> __device__ __forceinline__ float harmonic2<float>(float a, float b) {
+    return __fdividef(2.0f, a + b);
+}
+template <> __device__ __forceinline__ double harmonic2<double>(double a, double b) {
+    return 2.0 / (a + b);
 }
 
 // Row of the row-scaled Jacobi operator K = R A S (forward) or
@@ -191,7 +227,7 @@ __device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op,
     auto edge = [&](long long m, C2 F, bool nb_fixed) {
         if (ADJ && nb_fixed) return;
         const C4 r = op.rec[m];
-        const R g = R(2) / (me.x + r.x);
+        const R g = harmonic2<R>(me.x, r.x);
         C2 e = cscale(F, g);
         if (ADJ) e = cconj(e);
         C2 sv = cmul(make_c2<C2>(r.z, r.w), u[m]);
