@@ -223,6 +223,21 @@ int usv_basis_target_response(const void* basis, int64_t nx, int64_t ny, int64_t
                               int m, int basis_precision, const double* points, int p,
                               double dx, void* out, void* stream);
 
+/* ---- focal losses (phase_adjoint_optimizer.py:210-414) ------------------ */
+#define USV_LOSS_FOCAL_PRESSURE 0  /* FocalPressureLoss                            */
+#define USV_LOSS_FOCAL_CONTRAST 1  /* FocalContrastLoss (soft max over the mask)    */
+#define USV_LOSS_CONTRAST_RATIO 2  /* -mean_t |u_t|^2 / mean_mask |u|^2             */
+int usv_loss_workspace_bytes(int64_t n, size_t* bytes);
+/* value (device, 3 doubles): {loss, mean |u_t|, mean |u_t|^2}; cotangent
+ * (device complex128, N, may be NULL) in the dL = Re(g^H du) convention;
+ * mask: device bytes (1 = background / shell node) or NULL = every node;
+ * targets: device int64 Fortran node indices (repeats accumulate). Replaces
+ * FocalPressureLoss / FocalContrastLoss .evaluate_device. */
+int usv_loss(int mode, const void* field, int64_t n, const unsigned char* mask,
+             const int64_t* targets, int n_targets, double target_weight,
+             double background_weight, double temperature, double eps, double* value,
+             void* cotangent, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- gradients --------------------------------------------------------- */
 /* grad_rho, grad_c (device fp64) of dL = -Re(lambda^H dA u). */
 int usv_material_vjp(const usv_scene* scene, const void* op_buf, const double* rho,

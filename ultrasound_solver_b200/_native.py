@@ -26,6 +26,7 @@ USV_ERR_TOO_LARGE = 9
 FACE_REFLECTING, FACE_OPEN, FACE_SOFT, FACE_IMPEDANCE = 0, 1, 2, 3
 APPLY_A, APPLY_AH, APPLY_ABS_A, APPLY_ABS_AH, APPLY_K, APPLY_KH = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
+LOSS_FOCAL_PRESSURE, LOSS_FOCAL_CONTRAST, LOSS_CONTRAST_RATIO = 0, 1, 2
 
 
 class Scene(C.Structure):
@@ -88,6 +89,8 @@ _SIGNATURES = {
     "usv_basis_field": ([_P, _I64, _I, _I, _P, _P, _P], _I),
     "usv_basis_adjoint_workspace_bytes": ([_I64, _I, C.POINTER(_SZ)], _I),
     "usv_basis_adjoint": ([_P, _I64, _I, _I, _P, _P, _P, _P, _P, _SZ, _P], _I),
+    "usv_loss_workspace_bytes": ([_I64, C.POINTER(_SZ)], _I),
+    "usv_loss": ([_I, _P, _I64, _P, _P, _I, _D, _D, _D, _D, _P, _P, _P, _SZ, _P], _I),
     "usv_basis_adjoint_noalloc": ([_P, _I64, _I, _I, _P, _P, _P, _P, _P], _I),
     "usv_basis_target_response": ([_P, _I64, _I64, _I64, _I, _I, _P, _I, _D, _P, _P], _I),
 }

@@ -21,7 +21,7 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIBDIR = PKG / "_lib"
 LIBNAME = "libusv_b200.so"
-SOURCES = ("operator.cu", "gmres.cu", "scene.cu", "basis.cu")
+SOURCES = ("operator.cu", "gmres.cu", "scene.cu", "basis.cu", "losses.cu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
