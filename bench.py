@@ -41,7 +41,11 @@ FALLBACK_HBM_GBS = 6650.0
 # Inner iterations the row-scaled Jacobi GMRES(112) needs on this scene to
 # reach rtol 1e-9 (FP64 arm of this bench on a B200); the CPU sample below is
 # converted to solves/s with it because a full CPU solve takes hours.
-ITERATIONS_PER_SOLVE_FP64 = 30016
+ITERATIONS_PER_SOLVE_FP64 = 32816
+# DRAM bytes / algorithmic bytes of the Arnoldi kernels from one ncu capture
+# (profiles/arnoldi_kdots_korth_128cube_m112_j56.md); the roofline's `traffic`
+# is the algorithmic bytes per launch scaled by it.
+TRAFFIC_RATIO = {"arnoldi_dots": 1.02, "arnoldi_orth": 1.00}
 
 
 def parse_args(argv=None):
@@ -245,7 +249,9 @@ def run_ours(args):
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                        "peak_source": peak_kind, "unit": "GB/s",
                        "frac": achieved / peak if achieved else None,
-                       "traffic": None,
+                       "traffic": (d["bytes"] / max(d["launches"], 1) * TRAFFIC_RATIO[dom]
+                                   if dom in TRAFFIC_RATIO else None),
+                       "traffic_unit": "bytes per launch (ncu DRAM read+write)",
                        "avg_launch_us": 1000.0 * d["ms"] / max(d["launches"], 1),
                        "algorithmic_bytes_per_launch": d["bytes"] / max(d["launches"], 1),
                        "families": {k: {"launches": v["launches"], "ms": v["ms"],
