@@ -185,7 +185,6 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
 // needs no CTA barrier and holds no loads in registers.
 constexpr int kThreads = 256;
 constexpr int kPairs = 4;
-constexpr int kTU = 8;                          // basis vectors per CTA reduction
 constexpr int kChunk = 2 * kThreads * kPairs;  // 2048 nodes
 
 template <typename C2> struct Pipe {
@@ -325,15 +324,16 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
 // lanes over 16-byte pairs with kDotUnroll loads in flight, one warp reduction
 // per task; segments per vector grow when j is small so all warps work.
 constexpr int kDotUnroll = 8;
+constexpr int kDotsThreads = 512;
 
-template <typename R, bool ADJ>
-__global__ void __launch_bounds__(kThreads) k_dots(OpView<R> op, typename Tr<R>::c2* V, GState g,
-                                                   int j, Step step) {
+template <typename R, bool ADJ, int NT>
+__global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, typename Tr<R>::c2* V, GState g,
+                                                int j, Step step) {
     using C2 = typename Tr<R>::c2;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
     __shared__ __align__(16) C2 ys[kChunk];
-    __shared__ double2 segsum[USV_MAX_RESTART + 2][kThreads / 32];
+    __shared__ double2 segsum[USV_MAX_RESTART + 2 > NT / 16 ? USV_MAX_RESTART + 2 : NT / 16];
     const long long N = op.n;
     const long long n0 = (long long)blockIdx.x * kChunk;
     const int len = int(min((long long)kChunk, N - n0));
@@ -342,8 +342,9 @@ __global__ void __launch_bounds__(kThreads) k_dots(OpView<R> op, typename Tr<R>:
     C2* w = Vb + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
     Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-#pragma unroll 2
-    for (int e = threadIdx.x; e < kChunk; e += kThreads) {
+    constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
+#pragma unroll(kStencilUnroll)
+    for (int e = threadIdx.x; e < kChunk; e += NT) {
         C2 y = cmake<C2>(0.0, 0.0);
         if (e < len) {
             const long long n = n0 + e;
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(kThreads) k_dots(OpView<R> op, typename Tr<R>:
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int nw = kThreads / 32;
+    constexpr int nw = NT / 32;
     const int tasks_t = j + 2;  // t = 0..j dots, t = j+1: ||w||^2
     int segs = 1;
     while (segs < nw && tasks_t * segs < nw) segs <<= 1;
@@ -392,15 +393,15 @@ __global__ void __launch_bounds__(kThreads) k_dots(OpView<R> op, typename Tr<R>:
         }
         re = warp_sum(re);
         im = warp_sum(im);
-        if (lane == 0) segsum[t][seg] = make_double2(re, im);
+        if (lane == 0) segsum[task] = make_double2(re, im);
     }
     __syncthreads();
     double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * (g.m + 2);
-    for (int t = threadIdx.x; t < tasks_t; t += kThreads) {
+    for (int t = threadIdx.x; t < tasks_t; t += NT) {
         double re = 0.0, im = 0.0;
         for (int sg = 0; sg < segs; ++sg) {
-            re += segsum[t][sg].x;
-            im += segsum[t][sg].y;
+            re += segsum[t * segs + sg].x;
+            im += segsum[t * segs + sg].y;
         }
         if (t <= j) {
             const double st = g.sigma[b * (g.m + 1) + t];
@@ -709,6 +710,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     const size_t lsq_smem = sizeof(double2) * size_t(g.m) * (g.m + 1);
     const size_t pipe_smem = Pipe<C2>::UPP == 1 ? Pipe<C2>::BYTES : 16;
     const Step step = make_step(kThreads, s.nx, s.ny);
+    const Step step_d = make_step(kDotsThreads, s.nx, s.ny);
     USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(pipe_smem)));
     USV_CUDA_TRY(cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -750,7 +752,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         fam_bytes.clear();
         USV_CUDA_TRY(mark(st, k++, capturing));
         for (int j = 0; j < g.m; ++j) {
-            k_dots<R, ADJ><<<grid, kThreads, 0, st>>>(opk, V, g, j, step);
+            k_dots<R, ADJ, kDotsThreads><<<grid, kDotsThreads, 0, st>>>(opk, V, g, j, step_d);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
             // read u_0..u_j (u_j also feeds the stencil) + node record, write w
