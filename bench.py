@@ -61,6 +61,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GMRES comparator")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient timing")
     ap.add_argument("--cpu-iters", type=int, default=20)
     return ap.parse_args(argv)
 
@@ -291,6 +292,29 @@ def run_ours(args):
                       "h2d_bytes_per_step": int(rhs_host.nbytes),
                       "d2h_bytes_per_step": int(xh.nbytes), "steps": n_e2e,
                       "api": "HelmholtzB200Solver.solve_rhs(numpy)"}
+
+    # adjoint gradient: forward solve + A^H solve + phase VJP behind torch.autograd
+    if not args.no_adjoint:
+        from ultrasound_solver_b200.autograd import loss_of_field, phase_field
+        from ultrasound_solver_b200.losses import ContrastRatioLoss
+        it.precision, it.profile = "mixed", False
+        centre = (args.grid - 1) * solver.cfg.domain.dx / 2
+        loss = ContrastRatioLoss(solver.cfg, (centre, centre, 0.080), 0.006, 0.010)
+        ph = torch.tensor(solver.transducers.phases, dtype=torch.float64, device="cuda",
+                          requires_grad=True)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        L = loss_of_field(phase_field(ph, solver), loss)
+        L.backward()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_grad = max_over_ranks(e0.elapsed_time(e1), world)
+        out["adjoint_grad"] = {"value": world * 1000.0 / ms_grad, "unit": "adjoint grads/s",
+                               "ms_per_grad": ms_grad,
+                               "loss": "-|u_t|^2 / mean_shell |u|^2 (target 80 mm above the array)",
+                               "grad_norm": float(torch.linalg.norm(ph.grad).item())}
 
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_sample(args, cfg)
