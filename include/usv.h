@@ -79,6 +79,9 @@ extern "C" {
 /* precisions */
 #define USV_PREC_FP64 0      /* complex128 vectors, fp64 coefficients            */
 #define USV_PREC_MIXED 1     /* complex64 Krylov vectors + FP64 refinement       */
+#define USV_PREC_MIXED_BF16 2 /* bfloat16 complex Krylov vectors (4 B), fp32
+                                 stencil, FP64 dots/Hessenberg + FP64 refinement
+                                 (usv_gmres_* only)                              */
 
 typedef struct usv_scene {
     int32_t nx, ny, nz;

@@ -108,7 +108,7 @@ def test_contrast_ratio_cotangent_is_the_gradient(golden):
     assert abs(fd - an) <= 1e-6 * abs(an)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "bf16"])
 def test_autograd_phase_gradient(golden, precision):
     """Adjoint gradient through PhaseField vs central differences and the FP64 oracle adjoint."""
     from ultrasound_solver_b200.autograd import loss_of_field, phase_field

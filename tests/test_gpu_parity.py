@@ -56,7 +56,7 @@ def test_scaled_jacobi_operator(golden):
         np.testing.assert_allclose((jaca if adj else jac).cpu().numpy(), inv_d, rtol=1e-12)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "bf16"])
 def test_forward_solve_matches_direct(golden, precision):
     s = golden_solver(golden, precision=precision, gmres_rtol=1e-10, gmres_maxiter=20000)
     field = s.solve()
@@ -67,7 +67,7 @@ def test_forward_solve_matches_direct(golden, precision):
     assert it.last_iterations % 30 == 0
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "bf16"])
 def test_adjoint_solve_matches_direct(golden, precision):
     s = golden_solver(golden, precision=precision, gmres_rtol=1e-10, gmres_maxiter=20000)
     lam = s.solve_adjoint(golden["adj_rhs"])
@@ -85,8 +85,9 @@ def test_iteration_count_matches_restated_gmres(golden):
     assert abs(ours - ref.iterations) <= 30, (ours, ref.iterations)
 
 
-def test_batched_solve_matches_columns(golden):
-    s = golden_solver(golden, precision="mixed", gmres_rtol=1e-10, gmres_maxiter=20000)
+@pytest.mark.parametrize("precision", ["mixed", "bf16"])
+def test_batched_solve_matches_columns(golden, precision):
+    s = golden_solver(golden, precision=precision, gmres_rtol=1e-10, gmres_maxiter=20000)
     m = s.transducers.num_transducers
     rhs = s.sources.column_rhs(s.transducers.amplitudes)
     x = s.solve_rhs_device(rhs).cpu().numpy()

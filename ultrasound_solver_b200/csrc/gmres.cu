@@ -35,10 +35,11 @@ enum { ST_ACTIVE = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_NONFINITE = 3 };
 
 struct GState {
     int m, nblk, chunk, full_cycles, maxiter;
+    int nchunk;        // node chunks of `chunk` nodes; CTAs loop over them (grid <= nblk)
     long long n;
     long long nv;      // Krylov vector stride: n rounded up to 64 (512-B aligned pairs)
     double rtol;
-    double2* partial;  // [B][nblk][m+2]
+    double2* partial;  // [B][nblk][m+2], one slot per CTA of the launch
     double2* H;        // [B][m][m+1]  column j, rows 0..m
     double* gc;        // [B][m]
     double2* gs;       // [B][m]
@@ -110,6 +111,16 @@ __device__ __forceinline__ bool last_block_done(unsigned* counter, int nblk) {
 
 __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
 
+// Sum of the gridDim.x norm partials (slot 0) by the last CTA, in a fixed
+// order (thread-strided, then the block tree).
+__device__ __forceinline__ double reduce_slot0(const GState& g, int b, double* sh) {
+    double t = 0.0;
+    const double2* p = g.partial + (long long)b * g.nblk * (g.m + 2);
+    for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x)
+        t += ld_cg(p + (long long)q * (g.m + 2)).x;
+    return block_sum(t, sh);
+}
+
 // ------------------------------------------------------------ residual
 // r = Rs (rhs - OP x) in fp64 (OP = A or A^H); first=1: x = 0, r = Rs rhs.
 template <bool ADJ, typename C2>
@@ -119,33 +130,32 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
     const int b = blockIdx.y;
     if (!first && (g.status[b] != ST_ACTIVE)) return;
     __shared__ double sh[32];
-    const long long n0 = (long long)blockIdx.x * g.chunk;
-    const long long n1 = min(n0 + g.chunk, op.n);
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
     C2* v0 = V + (long long)b * (g.m + 1) * g.nv;
     double acc = 0.0;
-    Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-    for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
-        double2 r = rb[n];
-        if (!first) {
-            const double2 ax = a_row<ADJ ? USV_APPLY_AH : USV_APPLY_A>(op, xb, n, p);
-            r = csub(r, ax);
+    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+        const long long n0 = (long long)ch * g.chunk;
+        const long long n1 = min(n0 + g.chunk, op.n);
+        Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
+        for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+            double2 r = rb[n];
+            if (!first) {
+                const double2 ax = a_row<ADJ ? USV_APPLY_AH : USV_APPLY_A>(op, xb, n, p);
+                r = csub(r, ax);
+            }
+            advance(p, step, op.nx, op.ny);
+            r = cscale(r, op.rec[n].y);
+            const C2 rv = from_d<C2>(r);
+            v0[n] = rv;
+            acc += cabs2(to_d(rv));
         }
-        advance(p, step, op.nx, op.ny);
-        r = cscale(r, op.rec[n].y);
-        const C2 rv = from_d<C2>(r);
-        v0[n] = rv;
-        acc += cabs2(to_d(rv));
     }
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0)
         g.partial[((long long)b * g.nblk + blockIdx.x) * (g.m + 2)] = make_double2(acc, 0.0);
-    if (!last_block_done(&g.counter[b], g.nblk)) return;
-    double t = 0.0;
-    for (int q = threadIdx.x; q < g.nblk; q += blockDim.x)
-        t += ld_cg(&g.partial[((long long)b * g.nblk + q) * (g.m + 2)]).x;
-    t = block_sum(t, sh);
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    const double t = reduce_slot0(g, b, sh);
     if (threadIdx.x == 0) {
         const double beta = sqrt(t);
         if (first) {
@@ -188,7 +198,7 @@ constexpr int kPairs = 4;
 constexpr int kChunk = 2 * kThreads * kPairs;  // 2048 nodes
 
 template <typename C2> struct Pipe {
-    static constexpr int UPP = int(sizeof(C2) / 8);            // 16-B units per pair: 1 or 2
+    static constexpr int UPP = int(sizeof(C2) / 8);  // 16-B units per pair: 1, 2 (0: bf16 pairs)
     static constexpr int S = UPP == 1 ? 4 : 3;                  // stages
     static constexpr int STAGE_UNITS = kPairs * UPP * kThreads;
     static constexpr size_t BYTES = size_t(S) * STAGE_UNITS * 16;
@@ -261,6 +271,16 @@ __device__ __forceinline__ void ld_pair(const double2* p, double2& a, double2& b
     a = p[0];
     b = p[1];
 }
+__device__ __forceinline__ void st_pair(bf2* p, double2 a, double2 b) {
+    bf2 v[2] = {from_d<bf2>(a), from_d<bf2>(b)};
+    *reinterpret_cast<uint2*>(p) = *reinterpret_cast<const uint2*>(v);
+}
+__device__ __forceinline__ void ld_pair(const bf2* p, double2& a, double2& b) {
+    const uint2 raw = *reinterpret_cast<const uint2*>(p);
+    a = to_d(*reinterpret_cast<const bf2*>(&raw.x));
+    b = to_d(*reinterpret_cast<const bf2*>(&raw.y));
+}
+__device__ __forceinline__ double2 rounded(const bf2*, double2 a) { return to_d(from_d<bf2>(a)); }
 // value actually stored (rounded to the vector precision)
 __device__ __forceinline__ double2 rounded(const float2*, double2 a) {
     return make_double2(double(float(a.x)), double(float(a.y)));
@@ -272,8 +292,9 @@ __device__ __forceinline__ double2 rounded(const double2*, double2 a) { return a
 // through the cp.async pipeline (the caller has already issued the first
 // kStages-1 vectors when `prefetched`); complex128 uses direct 16-byte loads
 // unrolled over kUnroll vectors, which keeps enough bytes in flight with the
-// wider elements.
-constexpr int kUnroll = 2;
+// wider elements; bfloat16 pairs are 8-byte loads kept packed in registers
+// until use, four vectors in flight.
+template <typename C2> constexpr int kUnrollFor = sizeof(C2) == 4 ? 4 : 2;
 template <typename C2, typename F>
 __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long long nv, int last,
                                              int len, bool prefetched, F&& f) {
@@ -295,7 +316,31 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
                 for (int c = 0; c < 2; ++c) f(t, k, c, staged<C2>(stg, t, k, c));
         }
         cp_async_wait<0>();
+    } else if constexpr (sizeof(C2) == 4) {
+        constexpr int kUnroll = kUnrollFor<C2>;
+        for (int t0 = 0; t0 <= last; t0 += kUnroll) {
+            uint2 v[kUnroll][kPairs];
+#pragma unroll
+            for (int q = 0; q < kUnroll; ++q)
+#pragma unroll
+                for (int k = 0; k < kPairs; ++k) {
+                    const int e = 2 * (threadIdx.x + k * kThreads);
+                    v[q][k] = (t0 + q <= last && e < len)
+                                  ? *reinterpret_cast<const uint2*>(base + (long long)(t0 + q) * nv + e)
+                                  : make_uint2(0u, 0u);
+                }
+#pragma unroll
+            for (int q = 0; q < kUnroll; ++q)
+                if (t0 + q <= last) {
+#pragma unroll
+                    for (int k = 0; k < kPairs; ++k) {
+                        f(t0 + q, k, 0, to_d(*reinterpret_cast<const C2*>(&v[q][k].x)));
+                        f(t0 + q, k, 1, to_d(*reinterpret_cast<const C2*>(&v[q][k].y)));
+                    }
+                }
+        }
     } else {
+        constexpr int kUnroll = kUnrollFor<C2>;
         for (int t0 = 0; t0 <= last; t0 += kUnroll) {
             double2 v[kUnroll][kPairs][2];
 #pragma unroll
@@ -326,74 +371,80 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
 constexpr int kDotUnroll = 8;
 constexpr int kDotsThreads = 512;
 
-template <typename R, bool ADJ, int NT>
-__global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, typename Tr<R>::c2* V, GState g,
-                                                int j, Step step) {
-    using C2 = typename Tr<R>::c2;
+template <typename R, typename S, bool ADJ, int NT>
+__global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, int j, Step step) {
+    using C2 = S;  // stored vector element
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
     __shared__ __align__(16) C2 ys[kChunk];
     __shared__ double2 segsum[USV_MAX_RESTART + 2 > NT / 16 ? USV_MAX_RESTART + 2 : NT / 16];
     const long long N = op.n;
-    const long long n0 = (long long)blockIdx.x * kChunk;
-    const int len = int(min((long long)kChunk, N - n0));
     C2* Vb = V + (long long)b * (g.m + 1) * g.nv;
     const C2* uj = Vb + (long long)j * g.nv;
     C2* w = Vb + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
-    Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-    constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
-#pragma unroll(kStencilUnroll)
-    for (int e = threadIdx.x; e < kChunk; e += NT) {
-        C2 y = cmake<C2>(0.0, 0.0);
-        if (e < len) {
-            const long long n = n0 + e;
-            y = cscale(k_row<R, ADJ>(op, uj, n, p), sj);
-            w[n] = y;
-        }
-        ys[e] = y;
-        advance(p, step, op.nx, op.ny);
-    }
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nw = NT / 32;
     const int tasks_t = j + 2;  // t = 0..j dots, t = j+1: ||w||^2
     int segs = 1;
     while (segs < nw && tasks_t * segs < nw) segs <<= 1;
-    const int npairs = (len + 1) / 2;
-    const int per_seg = (npairs + segs - 1) / segs;
-    for (int task = warp; task < tasks_t * segs; task += nw) {
-        const int t = task / segs, seg = task % segs;
-        const int q0 = seg * per_seg, q1 = min(npairs, q0 + per_seg);
-        double re = 0.0, im = 0.0;
-        if (t <= j) {
-            const C2* ut = Vb + (long long)t * g.nv + n0;
-            for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
-                double2 a[kDotUnroll][2];
+    // each task belongs to one warp for every chunk: its sum accumulates in
+    // segsum in chunk order
+    for (int task = threadIdx.x; task < tasks_t * segs; task += NT)
+        segsum[task] = make_double2(0.0, 0.0);
+    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+        const long long n0 = (long long)ch * kChunk;
+        const int len = int(min((long long)kChunk, N - n0));
+        Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
+        __syncthreads();  // the previous chunk's dots are done with ys
+        constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
+#pragma unroll(kStencilUnroll)
+        for (int e = threadIdx.x; e < kChunk; e += NT) {
+            C2 y = from_d<C2>(make_double2(0.0, 0.0));
+            if (e < len) {
+                const long long n = n0 + e;
+                y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
+                w[n] = y;
+            }
+            ys[e] = y;
+            advance(p, step, op.nx, op.ny);
+        }
+        __syncthreads();
+        const int npairs = (len + 1) / 2;
+        const int per_seg = (npairs + segs - 1) / segs;
+        for (int task = warp; task < tasks_t * segs; task += nw) {
+            const int t = task / segs, seg = task % segs;
+            const int q0 = seg * per_seg, q1 = min(npairs, q0 + per_seg);
+            double re = 0.0, im = 0.0;
+            if (t <= j) {
+                const C2* ut = Vb + (long long)t * g.nv + n0;
+                for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
+                    double2 a[kDotUnroll][2];
 #pragma unroll
-                for (int u = 0; u < kDotUnroll; ++u) {
-                    const int q = qb + 32 * u;
-                    if (q < q1) ld_pair(ut + 2 * q, a[u][0], a[u][1]);
-                    else a[u][0] = a[u][1] = make_double2(0.0, 0.0);
-                }
+                    for (int u = 0; u < kDotUnroll; ++u) {
+                        const int q = qb + 32 * u;
+                        if (q < q1) ld_pair(ut + 2 * q, a[u][0], a[u][1]);
+                        else a[u][0] = a[u][1] = make_double2(0.0, 0.0);
+                    }
 #pragma unroll
-                for (int u = 0; u < kDotUnroll; ++u) {
-                    const int q = min(qb + 32 * u, npairs - 1);
+                    for (int u = 0; u < kDotUnroll; ++u) {
+                        const int q = min(qb + 32 * u, npairs - 1);
 #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
-                        const double2 y = to_d(ys[2 * q + c]);
-                        re = fma(a[u][c].x, y.x, fma(a[u][c].y, y.y, re));
-                        im = fma(a[u][c].x, y.y, fma(-a[u][c].y, y.x, im));
+                        for (int c = 0; c < 2; ++c) {
+                            const double2 y = to_d(ys[2 * q + c]);
+                            re = fma(a[u][c].x, y.x, fma(a[u][c].y, y.y, re));
+                            im = fma(a[u][c].x, y.y, fma(-a[u][c].y, y.x, im));
+                        }
                     }
                 }
+            } else {
+                for (int q = q0 + lane; q < q1; q += 32)
+                    re += cabs2(to_d(ys[2 * q])) + cabs2(to_d(ys[2 * q + 1]));
             }
-        } else {
-            for (int q = q0 + lane; q < q1; q += 32)
-                re += cabs2(to_d(ys[2 * q])) + cabs2(to_d(ys[2 * q + 1]));
+            re = warp_sum(re);
+            im = warp_sum(im);
+            if (lane == 0) segsum[task] = cadd(segsum[task], make_double2(re, im));
         }
-        re = warp_sum(re);
-        im = warp_sum(im);
-        if (lane == 0) segsum[task] = make_double2(re, im);
     }
     __syncthreads();
     double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * (g.m + 2);
@@ -410,22 +461,26 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, typename Tr<R>::c2
         }
         part[t] = make_double2(re, im);
     }
-    if (!last_block_done(&g.counter[b], g.nblk)) return;
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    const int nparts = int(gridDim.x);
     for (int t = warp; t <= j + 1; t += nw) {
-        double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+        double re0 = 0.0, im0 = 0.0;
         const double2* pt = g.partial + (long long)b * g.nblk * (g.m + 2) + t;
-        int q = lane;
-        for (; q + 32 < g.nblk; q += 64) {
-            const double2 p0 = ld_cg(pt + (long long)q * (g.m + 2));
-            const double2 p1 = ld_cg(pt + (long long)(q + 32) * (g.m + 2));
-            re0 += p0.x; im0 += p0.y; re1 += p1.x; im1 += p1.y;
+        for (int q0 = 0; q0 < nparts; q0 += 32 * 4) {
+            double2 pv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + 32 * u + lane;
+                pv[u] = q < nparts ? ld_cg(pt + (long long)q * (g.m + 2)) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                re0 += pv[u].x;
+                im0 += pv[u].y;
+            }
         }
-        if (q < g.nblk) {
-            const double2 p0 = ld_cg(pt + (long long)q * (g.m + 2));
-            re0 += p0.x; im0 += p0.y;
-        }
-        re0 = warp_sum(re0 + re1);
-        im0 = warp_sum(im0 + im1);
+        re0 = warp_sum(re0);
+        im0 = warp_sum(im0);
         if (lane == 0) {
             if (t <= j) g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
             else g.wnorm[b] = sqrt(re0);
@@ -434,24 +489,10 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, typename Tr<R>::c2
     if (threadIdx.x == 0) g.counter[b] = 0;
 }
 
-// Sum of the nblk norm partials (slot 0) by the last CTA.
-__device__ __forceinline__ double reduce_slot0(const GState& g, int b, double* sh) {
-    double t0 = 0.0, t1 = 0.0;
-    const double2* p = g.partial + (long long)b * g.nblk * (g.m + 2);
-    int q = threadIdx.x;
-    for (; q + kThreads < g.nblk; q += 2 * kThreads) {
-        t0 += ld_cg(p + (long long)q * (g.m + 2)).x;
-        t1 += ld_cg(p + (long long)(q + kThreads) * (g.m + 2)).x;
-    }
-    if (q < g.nblk) t0 += ld_cg(p + (long long)q * (g.m + 2)).x;
-    return block_sum(t0 + t1, sh);
-}
-
 // ------------------------------------------------------------ Arnoldi: orthogonalise + norm
-template <typename R>
-__global__ void __launch_bounds__(kThreads) k_orth(typename Tr<R>::c2* V, long long N, GState g,
-                                                   int j) {
-    using C2 = typename Tr<R>::c2;
+template <typename S>
+__global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, int j) {
+    using C2 = S;
     using P = Pipe<C2>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
@@ -463,38 +504,39 @@ __global__ void __launch_bounds__(kThreads) k_orth(typename Tr<R>::c2* V, long l
     const int m = g.m;
     for (int t = threadIdx.x; t <= j; t += kThreads)
         hs[t] = cscale(g.H[((long long)b * m + j) * (m + 1) + t], g.sigma[b * (m + 1) + t]);
-    const long long n0 = (long long)blockIdx.x * kChunk;
-    const int len = int(min((long long)kChunk, N - n0));
     C2* Vb = V + (long long)b * (m + 1) * g.nv;
-    C2* w = Vb + (long long)(j + 1) * g.nv + n0;
-    const C2* base = Vb + n0;
-    double2 u[kPairs][2];
-#pragma unroll
-    for (int k = 0; k < kPairs; ++k) {
-        const int e = 2 * (threadIdx.x + k * kThreads);
-        if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
-        else u[k][0] = u[k][1] = make_double2(0.0, 0.0);
-    }
     __syncthreads();  // hs visible
-    stream_basis<C2>(stg, base, g.nv, j, len, false, [&](int t, int k, int c, double2 vv) {
-        const double2 h = hs[t];
-        u[k][c].x -= h.x * vv.x - h.y * vv.y;
-        u[k][c].y -= h.x * vv.y + h.y * vv.x;
-    });
     double acc = 0.0;
+    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+        const long long n0 = (long long)ch * kChunk;
+        const int len = int(min((long long)kChunk, N - n0));
+        C2* w = Vb + (long long)(j + 1) * g.nv + n0;
+        double2 u[kPairs][2];
 #pragma unroll
-    for (int k = 0; k < kPairs; ++k) {
-        const int e = 2 * (threadIdx.x + k * kThreads);
-        if (e < len) {
-            st_pair(w + e, u[k][0], u[k][1]);
-            acc += cabs2(rounded(w, u[k][0]));
-            if (e + 1 < len) acc += cabs2(rounded(w, u[k][1]));
+        for (int k = 0; k < kPairs; ++k) {
+            const int e = 2 * (threadIdx.x + k * kThreads);
+            if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
+            else u[k][0] = u[k][1] = make_double2(0.0, 0.0);
+        }
+        stream_basis<C2>(stg, Vb + n0, g.nv, j, len, false, [&](int t, int k, int c, double2 vv) {
+            const double2 h = hs[t];
+            u[k][c].x -= h.x * vv.x - h.y * vv.y;
+            u[k][c].y -= h.x * vv.y + h.y * vv.x;
+        });
+#pragma unroll
+        for (int k = 0; k < kPairs; ++k) {
+            const int e = 2 * (threadIdx.x + k * kThreads);
+            if (e < len) {
+                st_pair(w + e, u[k][0], u[k][1]);
+                acc += cabs2(rounded(w, u[k][0]));
+                if (e + 1 < len) acc += cabs2(rounded(w, u[k][1]));
+            }
         }
     }
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0)
         g.partial[((long long)b * g.nblk + blockIdx.x) * (m + 2)] = make_double2(acc, 0.0);
-    if (!last_block_done(&g.counter[b], g.nblk)) return;
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
     const double beta = sqrt(reduce_slot0(g, b, sh));
     // stage column j and the previous rotations in shared memory
     double2* col = g.H + ((long long)b * m + j) * (m + 1);
@@ -589,11 +631,10 @@ __global__ void __launch_bounds__(128) k_lsq(GState g) {
 }
 
 // ------------------------------------------------------------ solution update (fp64)
-template <typename R>
-__global__ void __launch_bounds__(kThreads) k_update(OpView<double> op,
-                                                     const typename Tr<R>::c2* V, double2* x,
+template <typename S>
+__global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S* V, double2* x,
                                                      long long ld, GState g) {
-    using C2 = typename Tr<R>::c2;
+    using C2 = S;
     using P = Pipe<C2>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
@@ -602,27 +643,29 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op,
     const int L = g.len[b];
     for (int t = threadIdx.x; t < L; t += kThreads) ys[t] = g.y[(long long)b * g.m + t];
     const long long N = op.n;
-    const long long n0 = (long long)blockIdx.x * kChunk;
-    const int len = int(min((long long)kChunk, N - n0));
-    const C2* base = V + (long long)b * (g.m + 1) * g.nv + n0;
     __syncthreads();  // ys visible
-    double2 acc[kPairs][2];
+    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+        const long long n0 = (long long)ch * kChunk;
+        const int len = int(min((long long)kChunk, N - n0));
+        const C2* base = V + (long long)b * (g.m + 1) * g.nv + n0;
+        double2 acc[kPairs][2];
 #pragma unroll
-    for (int k = 0; k < kPairs; ++k) acc[k][0] = acc[k][1] = make_double2(0.0, 0.0);
-    stream_basis<C2>(stg, base, g.nv, L - 1, len, false, [&](int t, int k, int c, double2 vv) {
-        acc[k][c] = cadd(acc[k][c], cmul(ys[t], vv));
-    });
-    double2* xb = x + b * ld + n0;
+        for (int k = 0; k < kPairs; ++k) acc[k][0] = acc[k][1] = make_double2(0.0, 0.0);
+        stream_basis<C2>(stg, base, g.nv, L - 1, len, false, [&](int t, int k, int c, double2 vv) {
+            acc[k][c] = cadd(acc[k][c], cmul(ys[t], vv));
+        });
+        double2* xb = x + b * ld + n0;
 #pragma unroll
-    for (int k = 0; k < kPairs; ++k)
+        for (int k = 0; k < kPairs; ++k)
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int e = 2 * (threadIdx.x + k * kThreads) + c;
-            if (e < len) {
-                const double4 rc = op.rec[n0 + e];
-                xb[e] = cadd(xb[e], cmul(make_double2(rc.z, rc.w), acc[k][c]));
+            for (int c = 0; c < 2; ++c) {
+                const int e = 2 * (threadIdx.x + k * kThreads) + c;
+                if (e < len) {
+                    const double4 rc = op.rec[n0 + e];
+                    xb[e] = cadd(xb[e], cmul(make_double2(rc.z, rc.w), acc[k][c]));
+                }
             }
-        }
+    }
 }
 
 // ------------------------------------------------------------ final gates (fp64)
@@ -633,12 +676,11 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
                                                const double2* x, long long ld, GState g) {
     const int b = blockIdx.y;
     __shared__ double sh[32];
-    const long long n0 = (long long)blockIdx.x * g.chunk;
-    const long long n1 = min(n0 + g.chunk, op.n);
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
     double s2 = 0.0, b2 = 0.0, bwd = 0.0, bad = 0.0;
-    for (long long n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < op.n;
+         n += (long long)gridDim.x * blockDim.x) {
         const Node p = decode(n, op.nx, op.ny);
         const double2 ax = a_row<ADJ ? USV_APPLY_AH : USV_APPLY_A>(op, xb, n, p);
         const double2 den = a_row<ADJ ? USV_APPLY_ABS_AH : USV_APPLY_ABS_A>(op, xb, n, p);
@@ -660,9 +702,9 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
         part[0] = make_double2(s2, b2);
         part[1] = make_double2(bwd, bad);
     }
-    if (!last_block_done(&g.counter[b], g.nblk)) return;
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
     double ts = 0, tb = 0, tw = 0, tbad = 0;
-    for (int q = threadIdx.x; q < g.nblk; q += blockDim.x) {
+    for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x) {
         const double2* pq = g.partial + ((long long)b * g.nblk + q) * (g.m + 2);
         const double2 p0 = ld_cg(pq), p1 = ld_cg(pq + 1);
         ts += p0.x;
@@ -698,23 +740,43 @@ static cudaStream_t capture_stream() {
 }
 
 
-template <typename R, bool ADJ>
+template <typename R, typename S, bool ADJ>
 static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_params& p,
                      const double2* rhs, double2* x, int B, long long ld, char* ws,
                      const WsLayout& L, GState& g, usv_gmres_stats* stats, cudaStream_t strm) {
-    using C2 = typename Tr<R>::c2;
+    using C2 = S;  // stored Krylov vector element
     const OpView<double> op64 = make_view<double>(s, op_buf, ADJ);
     const OpView<R> opk = make_view<R>(s, op_buf, ADJ);
     C2* V = reinterpret_cast<C2*>(ws + L.V);
-    const dim3 grid(g.nblk, B);
     const size_t lsq_smem = sizeof(double2) * size_t(g.m) * (g.m + 1);
     const size_t pipe_smem = Pipe<C2>::UPP == 1 ? Pipe<C2>::BYTES : 16;
     const Step step = make_step(kThreads, s.nx, s.ny);
     const Step step_d = make_step(kDotsThreads, s.nx, s.ny);
-    USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(pipe_smem)));
-    USV_CUDA_TRY(cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    USV_CUDA_TRY(cudaFuncSetAttribute(k_update<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(pipe_smem)));
+    // Grids fill the GPU once (resident CTAs per SM x SMs, shared by the B
+    // right-hand sides); every CTA loops over node chunks, so there is no
+    // partial last wave and the last CTA reduces one partial per CTA.
+    int dev = 0, sms = 0;
+    USV_CUDA_TRY(cudaGetDevice(&dev));
+    USV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    auto grid_for = [&](const void* fn, int threads, size_t smem, dim3& grid) -> int {
+        int per_sm = 0;
+        USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+        long long x = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1) / B;
+        x = x < 1 ? 1 : (x > g.nchunk ? g.nchunk : x);
+        grid = dim3(unsigned(x), unsigned(B));
+        return USV_OK;
+    };
+    dim3 grid_res, grid_dots, grid_orth, grid_upd, grid_gates;
+    if (int e = grid_for((const void*)k_residual<ADJ, C2>, 256, 0, grid_res)) return e;
+    if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0, grid_dots))
+        return e;
+    if (int e = grid_for((const void*)k_orth<S>, kThreads, pipe_smem, grid_orth)) return e;
+    if (int e = grid_for((const void*)k_update<S>, kThreads, pipe_smem, grid_upd)) return e;
+    if (int e = grid_for((const void*)k_gates<ADJ>, 256, 0, grid_gates)) return e;
     if (lsq_smem > 48 * 1024)
         USV_CUDA_TRY(cudaFuncSetAttribute(k_lsq, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(lsq_smem)));
@@ -726,7 +788,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         USV_CUDA_TRY(cudaMemset2DAsync(V + g.n, g.nv * sizeof(C2), 0, (g.nv - g.n) * sizeof(C2),
                                        size_t(g.m + 1) * B, strm));
     USV_CUDA_TRY(cudaMemset2DAsync(x, ld * sizeof(double2), 0, g.n * sizeof(double2), B, strm));
-    k_residual<ADJ, C2><<<grid, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
+    k_residual<ADJ, C2><<<grid_res, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
     USV_CUDA_TRY(cudaGetLastError());
 
     // Event timing: one event before the first kernel of a cycle and one after
@@ -752,12 +814,12 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         fam_bytes.clear();
         USV_CUDA_TRY(mark(st, k++, capturing));
         for (int j = 0; j < g.m; ++j) {
-            k_dots<R, ADJ, kDotsThreads><<<grid, kDotsThreads, 0, st>>>(opk, V, g, j, step_d);
+            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
             // read u_0..u_j (u_j also feeds the stencil) + node record, write w
             fam_bytes.push_back(nn * (vb * (j + 2) + 4.0 * sizeof(R)));
-            k_orth<R><<<grid, kThreads, pipe_smem, st>>>(V, g.n, g, j);
+            k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(1);
             fam_bytes.push_back(nn * vb * (j + 3));
@@ -766,11 +828,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(2);
         fam_bytes.push_back(0.0);
-        k_update<R><<<grid, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
+        k_update<S><<<grid_upd, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(3);
         fam_bytes.push_back(nn * (vb * g.m + 2 * sizeof(double2) + sizeof(double4)));
-        k_residual<ADJ, C2><<<grid, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
+        k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(4);
         fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
@@ -835,7 +897,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         return rc;
     }
     if (prof) USV_CUDA_TRY(cudaEventRecord(ev[0], strm));
-    k_gates<ADJ><<<grid, 256, 0, strm>>>(op64, rhs, x, ld, g);
+    k_gates<ADJ><<<grid_gates, 256, 0, strm>>>(op64, rhs, x, ld, g);
     USV_CUDA_TRY(cudaGetLastError());
     if (prof) {
         USV_CUDA_TRY(cudaEventRecord(ev[1], strm));
@@ -881,6 +943,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     return USV_OK;
 }
 
+static size_t vector_bytes(int precision) {
+    return precision == USV_PREC_FP64 ? sizeof(double2)
+                                      : precision == USV_PREC_MIXED_BF16 ? sizeof(bf2) : sizeof(float2);
+}
+
 static int check_params(const usv_scene* scene, const usv_gmres_params* p, int nrhs,
                         long long* n, int* m, int* chunk, int* nblk) {
     if (!scene || !p || nrhs < 1 || nrhs > 65535) return USV_ERR_ARG;
@@ -889,7 +956,9 @@ static int check_params(const usv_scene* scene, const usv_gmres_params* p, int n
     if (p->restart < 1 || p->restart > USV_MAX_RESTART || p->maxiter < 0) return USV_ERR_ARG;
     if (p->history_capacity < 0) return USV_ERR_ARG;
     if (!(p->rtol >= 0) || !(p->backward_error_tol >= 0)) return USV_ERR_ARG;
-    if (p->precision != USV_PREC_FP64 && p->precision != USV_PREC_MIXED) return USV_ERR_ARG;
+    if (p->precision != USV_PREC_FP64 && p->precision != USV_PREC_MIXED &&
+        p->precision != USV_PREC_MIXED_BF16)
+        return USV_ERR_ARG;
     *m = int(p->restart < *n ? p->restart : *n);
     *chunk = kChunk;  // node chunk per CTA (block_nodes is reserved)
     if (p->block_nodes != 0 && p->block_nodes != kChunk) return USV_ERR_ARG;
@@ -910,7 +979,7 @@ int usv_gmres_workspace_bytes(const usv_scene* scene, const usv_gmres_params* pa
     int st = check_params(scene, params, nrhs, &n, &m, &chunk, &nblk);
     if (st) return st;
     if (!bytes) return USV_ERR_ARG;
-    const size_t vb = params->precision == USV_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+    const size_t vb = vector_bytes(params->precision);
     *bytes = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity).total;
     return USV_OK;
 }
@@ -923,13 +992,14 @@ int usv_gmres_solve(const usv_scene* scene, const void* op_buf, const usv_gmres_
     int st = check_params(scene, params, nrhs, &n, &m, &chunk, &nblk);
     if (st) return st;
     if (!op_buf || !rhs || !x || !workspace || !stats || ld < n) return USV_ERR_ARG;
-    const size_t vb = params->precision == USV_PREC_FP64 ? sizeof(double2) : sizeof(float2);
+    const size_t vb = vector_bytes(params->precision);
     const WsLayout L = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity);
     if (workspace_bytes < L.total) return USV_ERR_WORKSPACE;
     char* ws = static_cast<char*>(workspace);
     GState g{};
     g.m = m;
     g.nblk = nblk;
+    g.nchunk = nblk;
     g.chunk = chunk;
     g.full_cycles = params->full_cycles ? 1 : 0;
     g.maxiter = params->maxiter;
@@ -959,12 +1029,13 @@ int usv_gmres_solve(const usv_scene* scene, const void* op_buf, const usv_gmres_
     const double2* b = static_cast<const double2*>(rhs);
     double2* xx = static_cast<double2*>(x);
     const bool adj = params->adjoint != 0;
-    if (params->precision == USV_PREC_FP64) {
-        return adj ? run_gmres<double, true>(*scene, op_buf, *params, b, xx, nrhs, ld, ws, L, g, stats, strm)
-                   : run_gmres<double, false>(*scene, op_buf, *params, b, xx, nrhs, ld, ws, L, g, stats, strm);
-    }
-    return adj ? run_gmres<float, true>(*scene, op_buf, *params, b, xx, nrhs, ld, ws, L, g, stats, strm)
-               : run_gmres<float, false>(*scene, op_buf, *params, b, xx, nrhs, ld, ws, L, g, stats, strm);
+#define USV_RUN(R, S, A) run_gmres<R, S, A>(*scene, op_buf, *params, b, xx, nrhs, ld, ws, L, g, stats, strm)
+    if (params->precision == USV_PREC_FP64)
+        return adj ? USV_RUN(double, double2, true) : USV_RUN(double, double2, false);
+    if (params->precision == USV_PREC_MIXED_BF16)
+        return adj ? USV_RUN(float, bf2, true) : USV_RUN(float, bf2, false);
+    return adj ? USV_RUN(float, float2, true) : USV_RUN(float, float2, false);
+#undef USV_RUN
 }
 
 }  // extern "C"

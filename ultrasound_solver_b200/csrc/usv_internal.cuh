@@ -11,6 +11,7 @@
 // node coordinates, so no mask is stored.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -76,6 +77,31 @@ template <> __device__ __forceinline__ float2 from_d<float2>(double2 a) {
     return make_float2(float(a.x), float(a.y));
 }
 template <> __device__ __forceinline__ double2 from_d<double2>(double2 a) { return a; }
+
+// bfloat16 complex storage of Krylov vectors (USV_PREC_MIXED_BF16): 4 bytes per
+// value, widened to float for the stencil and to double for the dots.
+using bf2 = __nv_bfloat162;
+__device__ __forceinline__ double2 to_d(bf2 a) {
+    const float2 f = __bfloat1622float2(a);
+    return make_double2(f.x, f.y);
+}
+template <> __device__ __forceinline__ bf2 from_d<bf2>(double2 a) {
+    return __floats2bfloat162_rn(float(a.x), float(a.y));
+}
+// stored value S -> compute value C, and back
+template <typename C> __device__ __forceinline__ C widen(float2 a) { return cmake<C>(a.x, a.y); }
+template <typename C> __device__ __forceinline__ C widen(double2 a) { return cmake<C>(a.x, a.y); }
+template <typename C> __device__ __forceinline__ C widen(bf2 a) {
+    const float2 f = __bfloat1622float2(a);
+    return cmake<C>(f.x, f.y);
+}
+template <> __device__ __forceinline__ float2 widen<float2>(float2 a) { return a; }
+template <> __device__ __forceinline__ double2 widen<double2>(double2 a) { return a; }
+template <typename S> __device__ __forceinline__ S narrow(float2 a);
+template <typename S> __device__ __forceinline__ S narrow(double2 a);
+template <> __device__ __forceinline__ float2 narrow<float2>(float2 a) { return a; }
+template <> __device__ __forceinline__ double2 narrow<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ bf2 narrow<bf2>(float2 a) { return __float22bfloat162_rn(a); }
 
 // ---------------------------------------------------------------- layout
 // Byte offsets of the operator buffer. Everything is derived from the scene,
@@ -211,13 +237,12 @@ template <> __device__ __forceinline__ double harmonic2<double>(double a, double
 //   forward : y = u_n + R_n sum_j e_nj s_j u_j          (fixed row: y = u_n)
 //   adjoint : y = u_n + R'_n sum_{j not fixed} conj(e_nj) s'_j u_j
 // The unit diagonal follows from s = 1/(R A_ii) (iterative_solver.py:46-56).
-template <typename R, bool ADJ>
-__device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op,
-                                                    const typename Tr<R>::c2* __restrict__ u,
+template <typename R, bool ADJ, typename S = typename Tr<R>::c2>
+__device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op, const S* __restrict__ u,
                                                     long long n, Node p) {
     using C2 = typename Tr<R>::c2;
     using C4 = typename Tr<R>::c4;
-    const C2 un = u[n];
+    const C2 un = widen<C2>(u[n]);
     const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
     if (!ADJ && fixed) return un;
     const C4 me = op.rec[n];
@@ -230,7 +255,7 @@ __device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op,
         const R g = harmonic2<R>(me.x, r.x);
         C2 e = cscale(F, g);
         if (ADJ) e = cconj(e);
-        C2 sv = cmul(make_c2<C2>(r.z, r.w), u[m]);
+        C2 sv = cmul(make_c2<C2>(r.z, r.w), widen<C2>(u[m]));
         acc = cadd(acc, cmul(e, sv));
     };
     const long long sx = 1, sy = op.nx, sz = (long long)op.nx * op.ny;

@@ -9,8 +9,11 @@ batched over right-hand sides.
 
 precision="mixed": complex64 Krylov vectors and stencil inside each cycle,
 FP64 Gram-Schmidt dots, Hessenberg/Givens, true residual and solution update
-(iterative refinement at every restart). precision="fp64": complex128
-throughout — the plain FP64 comparator.
+(iterative refinement at every restart). precision="bf16": the same with the
+Krylov vectors stored as bfloat16 complex (4 bytes per node; the fp32
+stencil and FP64 dots widen them on load), which halves the basis traffic;
+the FP64 refinement at every restart keeps the converged solution the same.
+precision="fp64": complex128 throughout — the plain FP64 comparator.
 """
 from __future__ import annotations
 
@@ -21,6 +24,7 @@ import torch
 from . import _native as N
 
 _PRECISIONS = {"mixed": N.PREC_MIXED, "fp64": N.PREC_FP64, "complex64": N.PREC_MIXED,
+               "bf16": N.PREC_MIXED_BF16, "mixed_bf16": N.PREC_MIXED_BF16,
                "complex128": N.PREC_FP64}
 
 
