@@ -197,12 +197,26 @@ constexpr int kThreads = 256;
 constexpr int kPairs = 4;
 constexpr int kChunk = 2 * kThreads * kPairs;  // 2048 nodes
 
+// Per-thread node mapping and staging geometry by vector element size:
+//   complex128 (16 B): pair k = nodes 2(t + kThreads k) + {0,1}, two 16-B units
+//   complex64  (8 B) : same pairs, one 16-B unit per pair (cp.async staged)
+//   bfloat16   (4 B) : a 16-B unit holds 4 nodes; thread t owns units at nodes
+//                      4(t + kThreads u), u < kPairs/2, pair k = half k%2 of
+//                      unit k/2 (cp.async staged)
 template <typename C2> struct Pipe {
-    static constexpr int UPP = int(sizeof(C2) / 8);  // 16-B units per pair: 1, 2 (0: bf16 pairs)
-    static constexpr int S = UPP == 1 ? 4 : 3;                  // stages
-    static constexpr int STAGE_UNITS = kPairs * UPP * kThreads;
+    static constexpr int ES = int(sizeof(C2));
+    static constexpr bool STAGED = ES <= 8;                 // cp.async pipeline
+    static constexpr int UNITS = kPairs * 2 * ES / 16;      // 16-B units per thread per vector
+    static constexpr int S = ES == 4 ? 6 : (ES == 8 ? 4 : 3);  // stages
+    static constexpr int STAGE_UNITS = UNITS * kThreads;
     static constexpr size_t BYTES = size_t(S) * STAGE_UNITS * 16;
 };
+
+// First node (chunk-relative) of this thread's pair k.
+template <typename C2> __device__ __forceinline__ int pair_node(int k) {
+    if constexpr (sizeof(C2) == 4) return 4 * (threadIdx.x + kThreads * (k >> 1)) + 2 * (k & 1);
+    else return 2 * (threadIdx.x + kThreads * k);
+}
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
     const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -220,22 +234,21 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // Stage basis vector t (chunk at `base`, `len` valid nodes) into stage t % S;
 // slots of pairs outside the chunk (or t > last) are zero-filled, no read.
+// A unit that starts inside the chunk is copied whole: a bfloat16 unit may
+// run past the last node into the zeroed padding of the vector.
 template <typename C2>
 __device__ __forceinline__ void stage_vector(uint4* stg, const C2* base, int t, int last,
                                              int len) {
     using P = Pipe<C2>;
+    static_assert(P::STAGED, "complex128 is not staged");
     const int s = t % P::S;
     const char* src0 = reinterpret_cast<const char*>(base);
 #pragma unroll
-    for (int k = 0; k < kPairs; ++k) {
-        const int e = 2 * (threadIdx.x + k * kThreads);
+    for (int u = 0; u < P::UNITS; ++u) {
+        const int e = pair_node<C2>(P::ES == 4 ? 2 * u : u);
         const bool ok = t <= last && e < len;
-#pragma unroll
-        for (int h = 0; h < P::UPP; ++h) {
-            uint4* dst = stg + ((s * kPairs + k) * P::UPP + h) * kThreads + threadIdx.x;
-            const char* src = ok ? src0 + size_t(e) * sizeof(C2) + 16 * h : src0;
-            cp_async16(dst, src, ok ? 16 : 0);
-        }
+        uint4* dst = stg + (s * P::UNITS + u) * kThreads + threadIdx.x;
+        cp_async16(dst, ok ? src0 + size_t(e) * sizeof(C2) : src0, ok ? 16 : 0);
     }
     cp_async_commit();
 }
@@ -245,14 +258,19 @@ template <typename C2>
 __device__ __forceinline__ double2 staged(const uint4* stg, int t, int k, int c);
 template <>
 __device__ __forceinline__ double2 staged<float2>(const uint4* stg, int t, int k, int c) {
-    const int s = t % Pipe<float2>::S;
-    const float4 v = reinterpret_cast<const float4*>(stg)[(s * kPairs + k) * kThreads + threadIdx.x];
+    using P = Pipe<float2>;
+    const int s = t % P::S;
+    const float4 v = reinterpret_cast<const float4*>(stg)[(s * P::UNITS + k) * kThreads + threadIdx.x];
     return c ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
 }
 template <>
-__device__ __forceinline__ double2 staged<double2>(const uint4* stg, int t, int k, int c) {
-    const int s = t % Pipe<double2>::S;
-    return reinterpret_cast<const double2*>(stg)[((s * kPairs + k) * 2 + c) * kThreads + threadIdx.x];
+__device__ __forceinline__ double2 staged<bf2>(const uint4* stg, int t, int k, int c) {
+    using P = Pipe<bf2>;
+    const int s = t % P::S;
+    const unsigned* v = reinterpret_cast<const unsigned*>(
+        &stg[(s * P::UNITS + (k >> 1)) * kThreads + threadIdx.x]);
+    const unsigned raw = v[2 * (k & 1) + c];
+    return to_d(*reinterpret_cast<const bf2*>(&raw));
 }
 
 __device__ __forceinline__ void st_pair(float2* p, double2 a, double2 b) {
@@ -292,13 +310,12 @@ __device__ __forceinline__ double2 rounded(const double2*, double2 a) { return a
 // through the cp.async pipeline (the caller has already issued the first
 // kStages-1 vectors when `prefetched`); complex128 uses direct 16-byte loads
 // unrolled over kUnroll vectors, which keeps enough bytes in flight with the
-// wider elements; bfloat16 pairs are 8-byte loads kept packed in registers
-// until use, four vectors in flight.
-template <typename C2> constexpr int kUnrollFor = sizeof(C2) == 4 ? 4 : 2;
+// wider elements.
+template <typename C2> constexpr int kUnrollFor = 2;
 template <typename C2, typename F>
 __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long long nv, int last,
                                              int len, bool prefetched, F&& f) {
-    if constexpr (Pipe<C2>::UPP == 1) {
+    if constexpr (Pipe<C2>::STAGED) {
         using P = Pipe<C2>;
         auto issue = [&](int t) {
             stage_vector<C2>(stg, base + (long long)(t <= last ? t : 0) * nv, t, last, len);
@@ -316,29 +333,6 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
                 for (int c = 0; c < 2; ++c) f(t, k, c, staged<C2>(stg, t, k, c));
         }
         cp_async_wait<0>();
-    } else if constexpr (sizeof(C2) == 4) {
-        constexpr int kUnroll = kUnrollFor<C2>;
-        for (int t0 = 0; t0 <= last; t0 += kUnroll) {
-            uint2 v[kUnroll][kPairs];
-#pragma unroll
-            for (int q = 0; q < kUnroll; ++q)
-#pragma unroll
-                for (int k = 0; k < kPairs; ++k) {
-                    const int e = 2 * (threadIdx.x + k * kThreads);
-                    v[q][k] = (t0 + q <= last && e < len)
-                                  ? *reinterpret_cast<const uint2*>(base + (long long)(t0 + q) * nv + e)
-                                  : make_uint2(0u, 0u);
-                }
-#pragma unroll
-            for (int q = 0; q < kUnroll; ++q)
-                if (t0 + q <= last) {
-#pragma unroll
-                    for (int k = 0; k < kPairs; ++k) {
-                        f(t0 + q, k, 0, to_d(*reinterpret_cast<const C2*>(&v[q][k].x)));
-                        f(t0 + q, k, 1, to_d(*reinterpret_cast<const C2*>(&v[q][k].y)));
-                    }
-                }
-        }
     } else {
         constexpr int kUnroll = kUnrollFor<C2>;
         for (int t0 = 0; t0 <= last; t0 += kUnroll) {
@@ -347,7 +341,7 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
             for (int q = 0; q < kUnroll; ++q)
 #pragma unroll
                 for (int k = 0; k < kPairs; ++k) {
-                    const int e = 2 * (threadIdx.x + k * kThreads);
+                    const int e = pair_node<C2>(k);
                     if (t0 + q <= last && e < len)
                         ld_pair(base + (long long)(t0 + q) * nv + e, v[q][k][0], v[q][k][1]);
                     else
@@ -366,11 +360,46 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
 }
 
 // Dots of w with u_0..u_j: one warp per (basis vector, segment of the chunk),
-// lanes over 16-byte pairs with kDotUnroll loads in flight, one warp reduction
-// per task; segments per vector grow when j is small so all warps work.
+// lanes over groups of NL nodes (one 16-byte load for complex64 / bfloat16,
+// two for complex128) with kDotUnroll loads in flight, kept packed until use;
+// one warp reduction per task; segments per vector grow when j is small so
+// all warps work.
 constexpr int kDotUnroll = 8;
 constexpr int kDotsThreads = 512;
 
+template <typename C2> struct LaneLoad;
+template <> struct LaneLoad<bf2> {
+    static constexpr int NL = 4;
+    uint4 r;
+    __device__ __forceinline__ void load(const bf2* p) { r = *reinterpret_cast<const uint4*>(p); }
+    __device__ __forceinline__ void zero() { r = make_uint4(0u, 0u, 0u, 0u); }
+    __device__ __forceinline__ double2 get(int i) const {
+        const unsigned v = i == 0 ? r.x : i == 1 ? r.y : i == 2 ? r.z : r.w;
+        return to_d(*reinterpret_cast<const bf2*>(&v));
+    }
+};
+template <> struct LaneLoad<float2> {
+    static constexpr int NL = 2;
+    float4 r;
+    __device__ __forceinline__ void load(const float2* p) { r = *reinterpret_cast<const float4*>(p); }
+    __device__ __forceinline__ void zero() { r = make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ __forceinline__ double2 get(int i) const {
+        return i ? make_double2(r.z, r.w) : make_double2(r.x, r.y);
+    }
+};
+template <> struct LaneLoad<double2> {
+    static constexpr int NL = 2;
+    double2 a, b;
+    __device__ __forceinline__ void load(const double2* p) { a = p[0]; b = p[1]; }
+    __device__ __forceinline__ void zero() { a = b = make_double2(0.0, 0.0); }
+    __device__ __forceinline__ double2 get(int i) const { return i ? b : a; }
+};
+
+// Arnoldi step j, part 1: each CTA computes its chunk of w = sigma_j K u_j
+// (stencil) into shared and global memory, then the dots <sigma_t u_t, w>,
+// t <= j, and ||w||^2. (A separate stencil kernel ahead of a streaming dots
+// kernel measured 9% slower per iteration at 128^3: the extra launch and the
+// re-read of w cost more than the overlap of the two phases gains.)
 template <typename R, typename S, bool ADJ, int NT>
 __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, int j, Step step) {
     using C2 = S;  // stored vector element
@@ -395,8 +424,8 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
-        Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
         __syncthreads();  // the previous chunk's dots are done with ys
+        Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
         constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
 #pragma unroll(kStencilUnroll)
         for (int e = threadIdx.x; e < kChunk; e += NT) {
@@ -410,36 +439,39 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
             advance(p, step, op.nx, op.ny);
         }
         __syncthreads();
-        const int npairs = (len + 1) / 2;
-        const int per_seg = (npairs + segs - 1) / segs;
+        constexpr int NL = LaneLoad<C2>::NL;
+        const int ngroups = (len + NL - 1) / NL;  // ys and the vector padding are zero past len
+        const int per_seg = (ngroups + segs - 1) / segs;
         for (int task = warp; task < tasks_t * segs; task += nw) {
             const int t = task / segs, seg = task % segs;
-            const int q0 = seg * per_seg, q1 = min(npairs, q0 + per_seg);
+            const int q0 = seg * per_seg, q1 = min(ngroups, q0 + per_seg);
             double re = 0.0, im = 0.0;
             if (t <= j) {
                 const C2* ut = Vb + (long long)t * g.nv + n0;
                 for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
-                    double2 a[kDotUnroll][2];
+                    LaneLoad<C2> a[kDotUnroll];
 #pragma unroll
                     for (int u = 0; u < kDotUnroll; ++u) {
                         const int q = qb + 32 * u;
-                        if (q < q1) ld_pair(ut + 2 * q, a[u][0], a[u][1]);
-                        else a[u][0] = a[u][1] = make_double2(0.0, 0.0);
+                        if (q < q1) a[u].load(ut + NL * q);
+                        else a[u].zero();
                     }
 #pragma unroll
                     for (int u = 0; u < kDotUnroll; ++u) {
-                        const int q = min(qb + 32 * u, npairs - 1);
+                        const int q = min(qb + 32 * u, ngroups - 1);
 #pragma unroll
-                        for (int c = 0; c < 2; ++c) {
-                            const double2 y = to_d(ys[2 * q + c]);
-                            re = fma(a[u][c].x, y.x, fma(a[u][c].y, y.y, re));
-                            im = fma(a[u][c].x, y.y, fma(-a[u][c].y, y.x, im));
+                        for (int c = 0; c < NL; ++c) {
+                            const double2 y = to_d(ys[NL * q + c]);
+                            const double2 av = a[u].get(c);
+                            re = fma(av.x, y.x, fma(av.y, y.y, re));
+                            im = fma(av.x, y.y, fma(-av.y, y.x, im));
                         }
                     }
                 }
             } else {
                 for (int q = q0 + lane; q < q1; q += 32)
-                    re += cabs2(to_d(ys[2 * q])) + cabs2(to_d(ys[2 * q + 1]));
+#pragma unroll
+                    for (int c = 0; c < NL; ++c) re += cabs2(to_d(ys[NL * q + c]));
             }
             re = warp_sum(re);
             im = warp_sum(im);
@@ -514,7 +546,7 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
         double2 u[kPairs][2];
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
-            const int e = 2 * (threadIdx.x + k * kThreads);
+            const int e = pair_node<C2>(k);
             if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
             else u[k][0] = u[k][1] = make_double2(0.0, 0.0);
         }
@@ -525,7 +557,7 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
         });
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
-            const int e = 2 * (threadIdx.x + k * kThreads);
+            const int e = pair_node<C2>(k);
             if (e < len) {
                 st_pair(w + e, u[k][0], u[k][1]);
                 acc += cabs2(rounded(w, u[k][0]));
@@ -659,7 +691,7 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
         for (int k = 0; k < kPairs; ++k)
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                const int e = 2 * (threadIdx.x + k * kThreads) + c;
+                const int e = pair_node<C2>(k) + c;
                 if (e < len) {
                     const double4 rc = op.rec[n0 + e];
                     xb[e] = cadd(xb[e], cmul(make_double2(rc.z, rc.w), acc[k][c]));
@@ -749,7 +781,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     const OpView<R> opk = make_view<R>(s, op_buf, ADJ);
     C2* V = reinterpret_cast<C2*>(ws + L.V);
     const size_t lsq_smem = sizeof(double2) * size_t(g.m) * (g.m + 1);
-    const size_t pipe_smem = Pipe<C2>::UPP == 1 ? Pipe<C2>::BYTES : 16;
+    const size_t pipe_smem = Pipe<C2>::STAGED ? Pipe<C2>::BYTES : 16;
     const Step step = make_step(kThreads, s.nx, s.ny);
     const Step step_d = make_step(kDotsThreads, s.nx, s.ny);
     USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
