@@ -48,7 +48,7 @@
 extern "C" {
 #endif
 
-#define USV_ABI_VERSION 1
+#define USV_ABI_VERSION 2
 
 /* status codes */
 #define USV_OK 0
@@ -100,11 +100,13 @@ typedef struct usv_scene {
 /* Per-kernel-family device time of one solve, measured with CUDA events
  * recorded between the launches (also inside the captured cycle graph).
  * Families: 0 Arnoldi stencil+dots, 1 orthogonalisation+norm,
- * 2 least squares, 3 solution update, 4 FP64 residual, 5 final gates. */
-#define USV_KFAMILIES 6
+ * 2 least squares, 3 solution update, 4 FP64 residual, 5 final gates,
+ * 6 recycled-space kernels (new pair, projection, harmonic Ritz dots),
+ * 7 unused. `launches` counts measured intervals (a projection interval
+ * holds two kernels). */
+#define USV_KFAMILIES 8
 typedef struct usv_gmres_profile {
     int32_t launches[USV_KFAMILIES];
-    int32_t reserved;
     double milliseconds[USV_KFAMILIES];
     double bytes[USV_KFAMILIES];   /* algorithmic DRAM bytes, summed over launches */
 } usv_gmres_profile;
@@ -124,6 +126,11 @@ typedef struct usv_gmres_params {
                                     restart test after the first (the library's
                                     pr_norm callback values); may be NULL        */
     usv_gmres_profile* profile;  /* host; NULL = no event timing                 */
+    int32_t recycle;             /* k > 0: GCRO-DR(m, k), deflated restarting with
+                                    k harmonic Ritz vectors carried from cycle to
+                                    cycle (k <= min(16, m-1)); 0: plain GMRES(m) */
+    int32_t recycle_every;       /* recompute the recycled space after every n-th
+                                    cycle (0 or 1: every cycle)                  */
 } usv_gmres_params;
 
 typedef struct usv_gmres_stats {

@@ -39,12 +39,13 @@ class Scene(C.Structure):
                 ("reserved", C.c_int32)]
 
 
-KFAMILIES = 6
-KFAMILY_NAMES = ("arnoldi_dots", "arnoldi_orth", "lsq", "update", "residual", "gates")
+KFAMILIES = 8
+KFAMILY_NAMES = ("arnoldi_dots", "arnoldi_orth", "lsq", "update", "residual", "gates",
+                 "recycle", "unused")
 
 
 class GmresProfile(C.Structure):
-    _fields_ = [("launches", C.c_int32 * KFAMILIES), ("reserved", C.c_int32),
+    _fields_ = [("launches", C.c_int32 * KFAMILIES),
                 ("milliseconds", C.c_double * KFAMILIES), ("bytes", C.c_double * KFAMILIES)]
 
 
@@ -54,7 +55,8 @@ class GmresParams(C.Structure):
                 ("adjoint", C.c_int32), ("full_cycles", C.c_int32), ("use_graph", C.c_int32),
                 ("block_nodes", C.c_int32), ("history_capacity", C.c_int32),
                 ("history", C.POINTER(C.c_double)),
-                ("profile", C.POINTER(GmresProfile))]
+                ("profile", C.POINTER(GmresProfile)),
+                ("recycle", C.c_int32), ("recycle_every", C.c_int32)]
 
 
 class GmresStats(C.Structure):
@@ -121,7 +123,7 @@ def load(path: Path | None = None, build_if_missing: bool = False):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = res
-    if lib.usv_abi_version() != 1:
+    if lib.usv_abi_version() != 2:
         raise RuntimeError("libusv_b200 ABI version mismatch")
     if path is None:
         _lib = lib

@@ -21,7 +21,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIBDIR = PKG / "_lib"
 LIBNAME = "libusv_b200.so"
-SOURCES = ("operator.cu", "gmres.cu", "scene.cu", "basis.cu", "losses.cu")
+SOURCES = ("operator.cu", "gmres.cu", "scene.cu", "basis.cu", "losses.cu", "dense.cpp")
+HEADERS = ("usv_internal.cuh", "dense.h")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,7 +41,7 @@ def _stale(target: Path) -> bool:
     if not target.exists():
         return True
     newest = max(p.stat().st_mtime for p in [*(CSRC / s for s in SOURCES),
-                                              CSRC / "usv_internal.cuh", INCLUDE / "usv.h"])
+                                              *(CSRC / h for h in HEADERS), INCLUDE / "usv.h"])
     return target.stat().st_mtime < newest
 
 
@@ -59,6 +60,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for src in SOURCES:
         obj = objdir / (Path(src).stem + ".o")
         cmd = [nvcc, *common, "-c", str(CSRC / src), "-o", str(obj)]
+        if src.endswith(".cpp"):  # host dense algebra: plain complex arithmetic, finite data
+            cmd.insert(1, "-Xcompiler=-fcx-limited-range")
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))

@@ -25,6 +25,7 @@
 #include <cstring>
 #include <vector>
 
+#include "dense.h"
 #include "usv_internal.cuh"
 
 #define USV_MAX_RESTART 112  // keeps the m x (m+1) least-squares tile in shared memory
@@ -33,13 +34,30 @@ namespace usv {
 
 enum { ST_ACTIVE = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_NONFINITE = 3 };
 
+// Per-RHS control words of a recycled (GCRO-DR) cycle, written by the host
+// before each cycle.
+enum {
+    CW_KC = 0,      // recycled vectors used by this cycle (0 or k)
+    CW_PAIR,        // pair buffer (U, C) used by this cycle
+    CW_VBUF,        // Krylov buffer of this cycle
+    CW_COMBINE,     // 1: build pair CW_DST at the start of this cycle
+    CW_SRC_PAIR,    // pair used by the cycle whose data builds the new pair
+    CW_SRC_VBUF,    // its Krylov buffer
+    CW_SRC_KC,      // its recycled count
+    CW_DST,         // pair buffer written by the combine
+    kCtl
+};
+constexpr int kPairBufs = 3;   // pairs in use: this cycle's, the source cycle's, the new one
+constexpr int kVBufs = 2;      // Krylov buffers: this cycle's and the previous cycle's
+
 struct GState {
     int m, nblk, chunk, full_cycles, maxiter;
     int nchunk;        // node chunks of `chunk` nodes; CTAs loop over them (grid <= nblk)
+    int ps;            // partial-sum slots per CTA
     long long n;
     long long nv;      // Krylov vector stride: n rounded up to 64 (512-B aligned pairs)
     double rtol;
-    double2* partial;  // [B][nblk][m+2], one slot per CTA of the launch
+    double2* partial;  // [B][nblk][ps], one row per CTA of the launch
     double2* H;        // [B][m][m+1]  column j, rows 0..m
     double* gc;        // [B][m]
     double2* gs;       // [B][m]
@@ -58,16 +76,45 @@ struct GState {
     int* len;          // [B]
     int* ended;        // [B]
     unsigned* counter; // [B]
+    // recycling (GCRO-DR), kr > 0 only
+    int kr;            // recycled vectors k
+    int hb_len;        // doubles per RHS in the host-read block
+    long long vstride; // elements between the Krylov buffers (B (m+1) nv)
+    long long pstride; // elements between pair buffers (B k nv)
+    void* Ubuf;        // [kPairBufs][B][k][nv] U, K U = C
+    void* Cbuf;        // [kPairBufs][B][k][nv] C, orthonormal
+    int* ctl;          // [B][kCtl]
+    double2* coef;     // [B][k + m + 1][2k] combine coefficients
+    double* hb;        // [B][hb_len] read by the host after each cycle:
+                       //   raw G columns [m][m+1] complex, bd [m+1][k] complex,
+                       //   sigma [m+1], d [k], then len, kc
+    double* dU;        // [kPairBufs][B][k] 1/||U_i||
+    double2* alpha;    // [B][k] projection C^H r of the cycle's first residual
+    int* klast;        // [B] recycled count of the last finished cycle
+    int* started;      // [B]
 };
+
+// host-read block offsets (in doubles)
+__host__ __device__ __forceinline__ int hb_graw(int) { return 0; }
+__host__ __device__ __forceinline__ int hb_bd(int m) { return 2 * m * (m + 1); }
+__host__ __device__ __forceinline__ int hb_sigma(int m, int k) { return hb_bd(m) + 2 * (m + 1) * k; }
+__host__ __device__ __forceinline__ int hb_d(int m, int k) { return hb_sigma(m, k) + m + 1; }
+__host__ __device__ __forceinline__ int hb_tail(int m, int k) { return hb_d(m, k) + k; }
+__host__ __device__ __forceinline__ int hb_size(int m, int k) { return hb_tail(m, k) + 2; }
 
 struct WsLayout {
     size_t V, partial, H, gc, gs, g, y, sigma, bnorm, atol, wnorm, gates, hist, status, cycles,
         iters, len, ended, counter, state_begin, total;
+    size_t U, C, bpart, coef, hb, dU, alpha, klast, started, ctl;  // recycling
 };
 
 static long long padded(long long n) { return (n + 63) / 64 * 64; }
 
-static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes, int hcap) {
+// Partial-sum slots per CTA: m+2 for the Arnoldi dots, (m+1) k for the
+// recycled-space dots.
+static int partial_slots(int m, int k) { return k > 0 && (m + 1) * k > m + 2 ? (m + 1) * k : m + 2; }
+
+static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes, int hcap, int k) {
     WsLayout L{};
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -75,8 +122,16 @@ static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes,
         off = align_up(off + bytes);
         return o;
     };
-    L.V = take(vec_bytes * size_t(padded(n)) * size_t(m + 1) * size_t(B));
-    L.partial = take(sizeof(double2) * size_t(B) * nblk * (m + 2));
+    const size_t vecs = size_t(padded(n)) * vec_bytes;
+    L.V = take(vecs * size_t(m + 1) * size_t(B) * (k > 0 ? kVBufs : 1));
+    if (k > 0) {
+        L.U = take(vecs * size_t(k) * B * kPairBufs);
+        L.C = take(vecs * size_t(k) * B * kPairBufs);
+        L.coef = take(sizeof(double2) * size_t(B) * (k + m + 1) * 2 * k);
+        L.hb = take(sizeof(double) * size_t(B) * hb_size(m, k));
+        L.ctl = take(sizeof(int) * size_t(B) * kCtl);
+    }
+    L.partial = take(sizeof(double2) * size_t(B) * nblk * partial_slots(m, k));
     L.state_begin = off;
     L.H = take(sizeof(double2) * size_t(B) * m * (m + 1));
     L.gc = take(sizeof(double) * size_t(B) * m);
@@ -95,6 +150,12 @@ static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes,
     L.len = take(sizeof(int) * B);
     L.ended = take(sizeof(int) * B);
     L.counter = take(sizeof(unsigned) * B);
+    if (k > 0) {
+        L.dU = take(sizeof(double) * size_t(kPairBufs) * B * k);
+        L.alpha = take(sizeof(double2) * size_t(B) * k);
+        L.klast = take(sizeof(int) * B);
+        L.started = take(sizeof(int) * B);
+    }
     L.total = off;
     return L;
 }
@@ -115,24 +176,58 @@ __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
 // order (thread-strided, then the block tree).
 __device__ __forceinline__ double reduce_slot0(const GState& g, int b, double* sh) {
     double t = 0.0;
-    const double2* p = g.partial + (long long)b * g.nblk * (g.m + 2);
+    const double2* p = g.partial + (long long)b * g.nblk * g.ps;
     for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x)
-        t += ld_cg(p + (long long)q * (g.m + 2)).x;
+        t += ld_cg(p + (long long)q * g.ps).x;
     return block_sum(t, sh);
 }
 
+// Vectors of RHS b's current cycle: t < kc are the recycled C_t (and U_t for
+// the solution update), the others Krylov slots of the cycle's buffer.
+template <typename S> struct CycleBasis {
+    S* V;        // Krylov slot 0
+    const S* C;  // C_0 of the cycle's pair (kc > 0)
+    const S* U;  // U_0 of the cycle's pair (kc > 0)
+    int kc;
+    int pair;
+};
+template <typename S>
+__device__ __forceinline__ CycleBasis<S> cycle_basis(S* V, const GState& g, int b) {
+    CycleBasis<S> cb;
+    cb.V = V + (long long)b * (g.m + 1) * g.nv;
+    cb.C = cb.U = cb.V;
+    cb.kc = 0;
+    cb.pair = 0;
+    if (g.kr > 0) {
+        const int* cw = g.ctl + b * kCtl;
+        cb.V += cw[CW_VBUF] * g.vstride;
+        cb.kc = cw[CW_KC];
+        cb.pair = cw[CW_PAIR] > 0 ? cw[CW_PAIR] : 0;
+        const long long po = cb.pair * g.pstride + (long long)b * g.kr * g.nv;
+        cb.C = static_cast<const S*>(g.Cbuf) + po;
+        cb.U = static_cast<const S*>(g.Ubuf) + po;
+    }
+    return cb;
+}
+
 // ------------------------------------------------------------ residual
-// r = Rs (rhs - OP x) in fp64 (OP = A or A^H); first=1: x = 0, r = Rs rhs.
+// r = Rs (rhs - OP x) in fp64 (OP = A or A^H) into Krylov slot kc of the
+// cycle; first=1 (or, when recycling, the first call for this RHS): x = 0,
+// r = Rs rhs. Recycled cycles (kc > 0) also set up the fixed leading block of
+// G = [[D, B], [0, Hbar]]: columns t < kc are d_t e_t (identity rotations),
+// C slots have unit scale; the projection kernels then form beta.
 template <bool ADJ, typename C2>
 __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const double2* rhs,
                                                   const double2* x, long long ld, C2* V,
                                                   GState g, int first, Step step) {
     const int b = blockIdx.y;
+    if (g.kr > 0) first = !g.started[b];
     if (!first && (g.status[b] != ST_ACTIVE)) return;
     __shared__ double sh[32];
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
-    C2* v0 = V + (long long)b * (g.m + 1) * g.nv;
+    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    C2* v0 = cb.V + (long long)cb.kc * g.nv;
     double acc = 0.0;
     for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * g.chunk;
@@ -153,9 +248,11 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
     }
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0)
-        g.partial[((long long)b * g.nblk + blockIdx.x) * (g.m + 2)] = make_double2(acc, 0.0);
+        g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
     const double t = reduce_slot0(g, b, sh);
+    __shared__ int st_sh;
+    const int m = g.m, kc = cb.kc;
     if (threadIdx.x == 0) {
         const double beta = sqrt(t);
         if (first) {
@@ -163,9 +260,10 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
             g.atol[b] = g.rtol * beta;
             g.cycles[b] = 0;
             g.iters[b] = 0;
+            if (g.kr > 0) g.started[b] = 1;
         } else {
             g.cycles[b] += 1;
-            g.iters[b] += g.full_cycles ? g.m : g.len[b];
+            g.iters[b] += (g.full_cycles ? m : g.len[b]) - (g.kr > 0 ? g.klast[b] : 0);
             const int c = g.cycles[b] - 1;
             if (c < g.hcap) g.hist[(long long)b * g.hcap + c] = g.bnorm[b] > 0 ? beta / g.bnorm[b] : 0.0;
         }
@@ -174,14 +272,28 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
         else if (beta <= g.atol[b]) st = ST_CONVERGED;
         else if (g.iters[b] >= g.maxiter) st = ST_MAXITER;
         g.status[b] = st;
+        st_sh = st;
         if (st == ST_ACTIVE) {
-            g.sigma[b * (g.m + 1)] = 1.0 / beta;
-            g.g[b * (g.m + 1)] = make_double2(beta, 0.0);
-            for (int i = 1; i <= g.m; ++i) g.g[b * (g.m + 1) + i] = make_double2(0.0, 0.0);
-            g.len[b] = g.m;
+            g.sigma[b * (m + 1) + kc] = 1.0 / beta;
+            for (int i = 0; i <= m; ++i) g.g[b * (m + 1) + i] = make_double2(i == kc ? beta : 0.0, 0.0);
+            g.len[b] = m;
             g.ended[b] = 0;
         }
         g.counter[b] = 0;
+    }
+    if (kc > 0) {
+        __syncthreads();
+        if (st_sh != ST_ACTIVE) return;
+        const double* d = g.dU + ((long long)cb.pair * gridDim.y + b) * g.kr;
+        for (int idx = threadIdx.x; idx < kc * (m + 1); idx += blockDim.x) {
+            const int col = idx / (m + 1), row = idx % (m + 1);
+            g.H[((long long)b * m + col) * (m + 1) + row] = make_double2(row == col ? d[col] : 0.0, 0.0);
+        }
+        for (int t = threadIdx.x; t < kc; t += blockDim.x) {
+            g.sigma[b * (m + 1) + t] = 1.0;
+            g.gc[(long long)b * m + t] = 1.0;
+            g.gs[(long long)b * m + t] = make_double2(0.0, 0.0);
+        }
     }
 }
 
@@ -313,13 +425,14 @@ __device__ __forceinline__ double2 rounded(const double2*, double2 a) { return a
 // wider elements.
 template <typename C2> constexpr int kUnrollFor = 2;
 template <typename C2, typename F>
-__device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long long nv, int last,
-                                             int len, bool prefetched, F&& f) {
+__device__ __forceinline__ void stream_basis(uint4* stg, const C2* base0, const C2* base1,
+                                             int split, long long nv, int last, int len,
+                                             bool prefetched, F&& f) {
+    // vector t lives at (t < split ? base0 : base1) + t nv
+    auto vec = [&](int t) { return (t < split ? base0 : base1) + (long long)t * nv; };
     if constexpr (Pipe<C2>::STAGED) {
         using P = Pipe<C2>;
-        auto issue = [&](int t) {
-            stage_vector<C2>(stg, base + (long long)(t <= last ? t : 0) * nv, t, last, len);
-        };
+        auto issue = [&](int t) { stage_vector<C2>(stg, vec(t <= last ? t : 0), t, last, len); };
         if (!prefetched) {
 #pragma unroll
             for (int t = 0; t < P::S - 1; ++t) issue(t);
@@ -343,7 +456,7 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base, long lo
                 for (int k = 0; k < kPairs; ++k) {
                     const int e = pair_node<C2>(k);
                     if (t0 + q <= last && e < len)
-                        ld_pair(base + (long long)(t0 + q) * nv + e, v[q][k][0], v[q][k][1]);
+                        ld_pair(vec(t0 + q) + e, v[q][k][0], v[q][k][1]);
                     else
                         v[q][k][0] = v[q][k][1] = make_double2(0.0, 0.0);
                 }
@@ -400,17 +513,26 @@ template <> struct LaneLoad<double2> {
 // t <= j, and ||w||^2. (A separate stencil kernel ahead of a streaming dots
 // kernel measured 9% slower per iteration at 128^3: the extra launch and the
 // re-read of w cost more than the overlap of the two phases gains.)
+// proj = 1 (recycled cycles): no stencil; the dots alpha_t = <C_t, r> of the
+// cycle's first residual r (slot kc) with the recycled C_t, t < kc.
 template <typename R, typename S, bool ADJ, int NT>
-__global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, int j, Step step) {
+__global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, int j, Step step,
+                                                int proj) {
     using C2 = S;  // stored vector element
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    if (proj) {
+        if (cb.kc == 0) return;
+        j = cb.kc - 1;
+    } else if (j < cb.kc) {
+        return;
+    }
     __shared__ __align__(16) C2 ys[kChunk];
     __shared__ double2 segsum[USV_MAX_RESTART + 2 > NT / 16 ? USV_MAX_RESTART + 2 : NT / 16];
     const long long N = op.n;
-    C2* Vb = V + (long long)b * (g.m + 1) * g.nv;
-    const C2* uj = Vb + (long long)j * g.nv;
-    C2* w = Vb + (long long)(j + 1) * g.nv;
+    const C2* uj = cb.V + (long long)j * g.nv;
+    C2* w = cb.V + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nw = NT / 32;
@@ -425,18 +547,23 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
         __syncthreads();  // the previous chunk's dots are done with ys
-        Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-        constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
+        if (!proj) {
+            Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
+            constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
 #pragma unroll(kStencilUnroll)
-        for (int e = threadIdx.x; e < kChunk; e += NT) {
-            C2 y = from_d<C2>(make_double2(0.0, 0.0));
-            if (e < len) {
-                const long long n = n0 + e;
-                y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
-                w[n] = y;
+            for (int e = threadIdx.x; e < kChunk; e += NT) {
+                C2 y = from_d<C2>(make_double2(0.0, 0.0));
+                if (e < len) {
+                    const long long n = n0 + e;
+                    y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
+                    w[n] = y;
+                }
+                ys[e] = y;
+                advance(p, step, op.nx, op.ny);
             }
-            ys[e] = y;
-            advance(p, step, op.nx, op.ny);
+        } else {
+            for (int e = threadIdx.x; e < kChunk; e += NT)
+                ys[e] = e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0));
         }
         __syncthreads();
         constexpr int NL = LaneLoad<C2>::NL;
@@ -447,7 +574,7 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
             const int q0 = seg * per_seg, q1 = min(ngroups, q0 + per_seg);
             double re = 0.0, im = 0.0;
             if (t <= j) {
-                const C2* ut = Vb + (long long)t * g.nv + n0;
+                const C2* ut = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
                 for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
                     LaneLoad<C2> a[kDotUnroll];
 #pragma unroll
@@ -479,7 +606,7 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         }
     }
     __syncthreads();
-    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * (g.m + 2);
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
     for (int t = threadIdx.x; t < tasks_t; t += NT) {
         double re = 0.0, im = 0.0;
         for (int sg = 0; sg < segs; ++sg) {
@@ -497,13 +624,13 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     const int nparts = int(gridDim.x);
     for (int t = warp; t <= j + 1; t += nw) {
         double re0 = 0.0, im0 = 0.0;
-        const double2* pt = g.partial + (long long)b * g.nblk * (g.m + 2) + t;
+        const double2* pt = g.partial + (long long)b * g.nblk * g.ps + t;
         for (int q0 = 0; q0 < nparts; q0 += 32 * 4) {
             double2 pv[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int q = q0 + 32 * u + lane;
-                pv[u] = q < nparts ? ld_cg(pt + (long long)q * (g.m + 2)) : make_double2(0.0, 0.0);
+                pv[u] = q < nparts ? ld_cg(pt + (long long)q * g.ps) : make_double2(0.0, 0.0);
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -514,20 +641,29 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         re0 = warp_sum(re0);
         im0 = warp_sum(im0);
         if (lane == 0) {
-            if (t <= j) g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
-            else g.wnorm[b] = sqrt(re0);
+            if (t > j) g.wnorm[b] = sqrt(re0);
+            else if (proj) g.alpha[(long long)b * g.kr + t] = make_double2(re0, im0);
+            else g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
         }
     }
     if (threadIdx.x == 0) g.counter[b] = 0;
 }
 
 // ------------------------------------------------------------ Arnoldi: orthogonalise + norm
+// proj = 1 (recycled cycles): r -= sum_t alpha_t C_t on the cycle's first
+// residual (slot kc), then beta = ||r|| starts the Krylov part of the cycle.
 template <typename S>
-__global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, int j) {
+__global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, int j, int proj) {
     using C2 = S;
-    using P = Pipe<C2>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    if (proj) {
+        if (cb.kc == 0) return;
+        j = cb.kc - 1;
+    } else if (j < cb.kc) {
+        return;
+    }
     extern __shared__ __align__(16) uint4 stg[];
     __shared__ double2 hs[USV_MAX_RESTART + 2];
     __shared__ double2 gsS[USV_MAX_RESTART + 1];
@@ -535,14 +671,14 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     __shared__ double sh[32];
     const int m = g.m;
     for (int t = threadIdx.x; t <= j; t += kThreads)
-        hs[t] = cscale(g.H[((long long)b * m + j) * (m + 1) + t], g.sigma[b * (m + 1) + t]);
-    C2* Vb = V + (long long)b * (m + 1) * g.nv;
+        hs[t] = proj ? g.alpha[(long long)b * g.kr + t]
+                     : cscale(g.H[((long long)b * m + j) * (m + 1) + t], g.sigma[b * (m + 1) + t]);
     __syncthreads();  // hs visible
     double acc = 0.0;
     for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
-        C2* w = Vb + (long long)(j + 1) * g.nv + n0;
+        C2* w = cb.V + (long long)(j + 1) * g.nv + n0;
         double2 u[kPairs][2];
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
@@ -550,7 +686,8 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
             if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
             else u[k][0] = u[k][1] = make_double2(0.0, 0.0);
         }
-        stream_basis<C2>(stg, Vb + n0, g.nv, j, len, false, [&](int t, int k, int c, double2 vv) {
+        stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
+                         [&](int t, int k, int c, double2 vv) {
             const double2 h = hs[t];
             u[k][c].x -= h.x * vv.x - h.y * vv.y;
             u[k][c].y -= h.x * vv.y + h.y * vv.x;
@@ -567,9 +704,24 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     }
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0)
-        g.partial[((long long)b * g.nblk + blockIdx.x) * (m + 2)] = make_double2(acc, 0.0);
+        g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
     const double beta = sqrt(reduce_slot0(g, b, sh));
+    if (proj) {
+        if (threadIdx.x == 0) {
+            g.counter[b] = 0;
+            const int kc = cb.kc;
+            if (beta > 1e-300 && isfinite(beta)) {
+                g.g[b * (m + 1) + kc] = make_double2(beta, 0.0);
+                g.sigma[b * (m + 1) + kc] = 1.0 / beta;
+            } else {  // r lies in span(C): the projection alone solves this cycle
+                g.g[b * (m + 1) + kc] = make_double2(0.0, 0.0);
+                g.len[b] = kc;
+                g.ended[b] = 1;
+            }
+        }
+        return;
+    }
     // stage column j and the previous rotations in shared memory
     double2* col = g.H + ((long long)b * m + j) * (m + 1);
     for (int t = threadIdx.x; t <= j; t += kThreads) {
@@ -580,6 +732,14 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
         }
     }
     __syncthreads();
+    if (g.kr > 0) {  // raw column of G (before the rotations) for the harmonic Ritz step
+        double* gr = g.hb + (long long)b * g.hb_len + hb_graw(m) + 2LL * j * (m + 1);
+        for (int t = threadIdx.x; t <= j + 1; t += kThreads) {
+            const double2 v = t <= j ? hs[t] : make_double2(beta, 0.0);
+            gr[2 * t] = v.x;
+            gr[2 * t + 1] = v.y;
+        }
+    }
     if (threadIdx.x == 0) {
         g.counter[b] = 0;
         hs[j + 1] = make_double2(beta, 0.0);
@@ -658,8 +818,28 @@ __global__ void __launch_bounds__(128) k_lsq(GState g) {
         if (threadIdx.x == 0) gv[k] = yk;
         __syncthreads();
     }
+    if (g.kr == 0) {
+        for (int i = threadIdx.x; i < L; i += blockDim.x)
+            g.y[(long long)b * m + i] = cscale(gv[i], g.sigma[b * (m + 1) + i]);
+        return;
+    }
+    // Recycled cycle: y_t (t < kc) multiplies Ut_t = d_t U_t, and the
+    // projection x += U alpha of the cycle's first residual is folded in.
+    const int* cw = g.ctl + b * kCtl;
+    const int kc = cw[CW_KC], pair = cw[CW_PAIR] > 0 ? cw[CW_PAIR] : 0;
+    const double* d = g.dU + ((long long)pair * gridDim.x + b) * g.kr;
     for (int i = threadIdx.x; i < L; i += blockDim.x)
-        g.y[(long long)b * m + i] = cscale(gv[i], g.sigma[b * (m + 1) + i]);
+        g.y[(long long)b * m + i] =
+            i < kc ? cadd(cscale(gv[i], d[i]), g.alpha[(long long)b * g.kr + i])
+                   : cscale(gv[i], g.sigma[b * (m + 1) + i]);
+    double* hb = g.hb + (long long)b * g.hb_len;
+    for (int i = threadIdx.x; i <= m; i += blockDim.x) hb[hb_sigma(m, g.kr) + i] = g.sigma[b * (m + 1) + i];
+    for (int i = threadIdx.x; i < g.kr; i += blockDim.x) hb[hb_d(m, g.kr) + i] = i < kc ? d[i] : 0.0;
+    if (threadIdx.x == 0) {
+        hb[hb_tail(m, g.kr)] = double(L);
+        hb[hb_tail(m, g.kr) + 1] = double(kc);
+        g.klast[b] = kc;
+    }
 }
 
 // ------------------------------------------------------------ solution update (fp64)
@@ -675,15 +855,17 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
     const int L = g.len[b];
     for (int t = threadIdx.x; t < L; t += kThreads) ys[t] = g.y[(long long)b * g.m + t];
     const long long N = op.n;
+    // solution vectors: U_t (t < kc) of the cycle's pair, then Krylov slots
+    const CycleBasis<C2> cb = cycle_basis(const_cast<C2*>(V), g, b);
     __syncthreads();  // ys visible
     for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
-        const C2* base = V + (long long)b * (g.m + 1) * g.nv + n0;
         double2 acc[kPairs][2];
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) acc[k][0] = acc[k][1] = make_double2(0.0, 0.0);
-        stream_basis<C2>(stg, base, g.nv, L - 1, len, false, [&](int t, int k, int c, double2 vv) {
+        stream_basis<C2>(stg, cb.U + n0, cb.V + n0, cb.kc, g.nv, L - 1, len, false,
+                         [&](int t, int k, int c, double2 vv) {
             acc[k][c] = cadd(acc[k][c], cmul(ys[t], vv));
         });
         double2* xb = x + b * ld + n0;
@@ -698,6 +880,173 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
                 }
             }
     }
+}
+
+// ------------------------------------------------------------ recycled space (GCRO-DR)
+constexpr int kMaxRecycle = 16;
+constexpr int kBdTile = 512;  // nodes of U staged in shared memory per pass
+
+template <typename S> struct Wide { using T = float2; };
+template <> struct Wide<double2> { using T = double2; };
+
+// bd[s][i] = <Vhat_s, Ut_i>, s <= m, i < kc: Vhat = [C_0..C_kc-1, sigma_s V_s],
+// Ut_i = d_i U_i (the columns of Vhat^H W that are not identity), written to
+// the host-read block. Each CTA stages a tile of U in shared memory; warp w
+// owns the slots s = w (mod warps) for every tile, so the per-CTA sums are
+// accumulated in a fixed order; the last CTA reduces the CTA partials.
+template <typename S>
+__global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g) {
+    using T = typename Wide<S>::T;
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
+    const CycleBasis<S> cb = cycle_basis(V, g, b);
+    const int kc = cb.kc, m = g.m;
+    if (kc == 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ut = reinterpret_cast<T*>(smem_raw);                                  // [kc][kBdTile]
+    double2* tab = reinterpret_cast<double2*>(ut + (size_t)kc * kBdTile);    // [m+1][kc]
+    for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) tab[q] = make_double2(0.0, 0.0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nw = kThreads / 32;
+    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+        for (int t0 = 0; t0 < kChunk; t0 += kBdTile) {
+            const long long n0 = (long long)ch * kChunk + t0;
+            const int len = int(max(0LL, min((long long)kBdTile, N - n0)));
+            __syncthreads();
+            for (int q = threadIdx.x; q < kc * kBdTile; q += kThreads) {
+                const int i = q / kBdTile, e = q % kBdTile;
+                ut[q] = e < len ? widen<T>(cb.U[(long long)i * g.nv + n0 + e]) : cmake<T>(0.0, 0.0);
+            }
+            __syncthreads();
+            for (int sl = warp; sl <= m; sl += nw) {
+                const S* vs = (sl < kc ? cb.C : cb.V) + (long long)sl * g.nv + n0;
+                T acc[kMaxRecycle];
+#pragma unroll
+                for (int i = 0; i < kMaxRecycle; ++i) acc[i] = cmake<T>(0.0, 0.0);
+                for (int e = lane; e < len; e += 32) {
+                    const T v = widen<T>(vs[e]);
+#pragma unroll
+                    for (int i = 0; i < kMaxRecycle; ++i)
+                        if (i < kc) {
+                            const T u = ut[i * kBdTile + e];
+                            acc[i].x += v.x * u.x + v.y * u.y;
+                            acc[i].y += v.x * u.y - v.y * u.x;
+                        }
+                }
+#pragma unroll
+                for (int i = 0; i < kMaxRecycle; ++i)
+                    if (i < kc) {
+                        const double re = warp_sum(double(acc[i].x));
+                        const double im = warp_sum(double(acc[i].y));
+                        if (lane == 0) tab[sl * kc + i] = cadd(tab[sl * kc + i], make_double2(re, im));
+                    }
+            }
+        }
+    }
+    __syncthreads();
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+    for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) part[q] = tab[q];
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    const double* d = g.dU + ((long long)cb.pair * gridDim.y + b) * g.kr;
+    double* out = g.hb + (long long)b * g.hb_len + hb_bd(m);
+    for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) {
+        double re = 0.0, im = 0.0;
+        const double2* pq = g.partial + (long long)b * g.nblk * g.ps + q;
+        for (int c = 0; c < int(gridDim.x); ++c) {
+            const double2 v = ld_cg(pq + (long long)c * g.ps);
+            re += v.x;
+            im += v.y;
+        }
+        const int sl = q / kc, i = q % kc;
+        const double sc = (sl < kc ? 1.0 : g.sigma[b * (m + 1) + sl]) * d[i];
+        out[2 * (sl + (m + 1) * i)] = re * sc;
+        out[2 * (sl + (m + 1) * i) + 1] = im * sc;
+    }
+    if (threadIdx.x == 0) g.counter[b] = 0;
+}
+
+// New recycled pair at the start of a cycle (when CW_COMBINE is set), from the
+// data of an earlier cycle: U' = [Ut, V_p] P R^{-1}, C' = [C, V_{p+1}] Q with
+// the coefficients (sigma, d folded in) from the host's harmonic Ritz step.
+// Inputs: the source pair U_0..U_{kc-1}, C_0..C_{kc-1} and the source Krylov
+// slots kc..m; coefficient rows in that order, columns U'_0..U'_{k-1},
+// C'_0..C'_{k-1}. Outputs go to a third pair buffer (no aliasing). Also
+// d'_i = 1/||U'_i|| for the new pair.
+template <typename S>
+__global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState g) {
+    using T = typename Wide<S>::T;
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE) return;
+    const int* cw = g.ctl + b * kCtl;
+    if (!cw[CW_COMBINE]) return;
+    const int m = g.m, k = g.kr, skc = cw[CW_SRC_KC];
+    const int rows = skc + m + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* cf = reinterpret_cast<T*>(smem_raw);  // [rows][2k]
+    __shared__ double sh[32];
+    for (int q = threadIdx.x; q < rows * 2 * k; q += kThreads) {
+        const double2 c = g.coef[(long long)b * (k + m + 1) * 2 * k + q];
+        cf[q] = cmake<T>(c.x, c.y);
+    }
+    const long long sp = (cw[CW_SRC_PAIR] > 0 ? cw[CW_SRC_PAIR] : 0) * g.pstride + (long long)b * k * g.nv;
+    const long long dp = cw[CW_DST] * g.pstride + (long long)b * k * g.nv;
+    const S* Uo = static_cast<const S*>(g.Ubuf) + sp;
+    const S* Co = static_cast<const S*>(g.Cbuf) + sp;
+    S* Un = static_cast<S*>(g.Ubuf) + dp;
+    S* Cn = static_cast<S*>(g.Cbuf) + dp;
+    const S* Vs = V + cw[CW_SRC_VBUF] * g.vstride + (long long)b * (m + 1) * g.nv;
+    __syncthreads();
+    double nrm[kMaxRecycle];
+#pragma unroll
+    for (int i = 0; i < kMaxRecycle; ++i) nrm[i] = 0.0;
+    for (long long n = (long long)blockIdx.x * kThreads + threadIdx.x; n < N;
+         n += (long long)gridDim.x * kThreads) {
+        for (int pass = 0; pass < 2; ++pass) {  // 0: U', 1: C'
+            T acc[kMaxRecycle];
+#pragma unroll
+            for (int i = 0; i < kMaxRecycle; ++i) acc[i] = cmake<T>(0.0, 0.0);
+            const int r_end = pass == 0 ? rows - 1 : rows;  // U' does not use slot m
+            for (int r = 0; r < r_end; ++r) {
+                if (pass == 0 && r >= skc && r < 2 * skc) continue;  // C rows feed C' only
+                if (pass == 1 && r < skc) continue;                  // U rows feed U' only
+                const S* src = r < skc ? Uo + (long long)r * g.nv
+                             : r < 2 * skc ? Co + (long long)(r - skc) * g.nv
+                                           : Vs + (long long)(r - skc) * g.nv;
+                const T v = widen<T>(src[n]);
+                const T* crow = cf + r * 2 * k + pass * k;
+#pragma unroll
+                for (int i = 0; i < kMaxRecycle; ++i)
+                    if (i < k) {
+                        const T c = crow[i];
+                        acc[i].x += c.x * v.x - c.y * v.y;
+                        acc[i].y += c.x * v.y + c.y * v.x;
+                    }
+            }
+            S* dst = pass == 0 ? Un : Cn;
+#pragma unroll
+            for (int i = 0; i < kMaxRecycle; ++i)
+                if (i < k) {
+                    const S o = narrow<S>(acc[i]);
+                    dst[(long long)i * g.nv + n] = o;
+                    if (pass == 0) nrm[i] += cabs2(to_d(o));
+                }
+        }
+    }
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+#pragma unroll
+    for (int i = 0; i < kMaxRecycle; ++i)
+        if (i < k) {
+            const double t = block_sum(nrm[i], sh);
+            if (threadIdx.x == 0) part[i] = make_double2(t, 0.0);
+        }
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    for (int i = threadIdx.x; i < k; i += kThreads) {
+        double t = 0.0;
+        const double2* pq = g.partial + (long long)b * g.nblk * g.ps + i;
+        for (int c = 0; c < int(gridDim.x); ++c) t += ld_cg(pq + (long long)c * g.ps).x;
+        g.dU[((long long)cw[CW_DST] * gridDim.y + b) * k + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
+    }
+    if (threadIdx.x == 0) g.counter[b] = 0;
 }
 
 // ------------------------------------------------------------ final gates (fp64)
@@ -729,7 +1078,7 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
     b2 = block_sum(b2, sh);
     bad = block_sum(bad, sh);
     bwd = block_max(isnan(bwd) ? INFINITY : bwd, sh);
-    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * (g.m + 2);
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
     if (threadIdx.x == 0) {
         part[0] = make_double2(s2, b2);
         part[1] = make_double2(bwd, bad);
@@ -737,7 +1086,7 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
     double ts = 0, tb = 0, tw = 0, tbad = 0;
     for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x) {
-        const double2* pq = g.partial + ((long long)b * g.nblk + q) * (g.m + 2);
+        const double2* pq = g.partial + ((long long)b * g.nblk + q) * g.ps;
         const double2 p0 = ld_cg(pq), p1 = ld_cg(pq + 1);
         ts += p0.x;
         tb += p0.y;
@@ -771,6 +1120,80 @@ static cudaStream_t capture_stream() {
     return s;
 }
 
+
+// Coefficients of the next recycled pair from one finished cycle's host-read
+// block: the harmonic Ritz update of GCRO-DR (Parks, de Sturler, Mackey,
+// Johnson & Maiti, SIAM J. Sci. Comput. 28 (2006), Algorithm 2.1) on
+//   G ((L+1) x L): columns t < kc = d_t e_t, columns t >= kc = the raw
+//                  Arnoldi columns (K W = Vhat G, W = [Ut, V_kc..V_{L-1}]),
+//   Vhat^H W:      columns t < kc = bd[:, t], columns t >= kc = e_t.
+// P = the k harmonic Ritz vectors of smallest |theta|, [Q, Rq] = qr(G P),
+// U' = W P Rq^{-1}, C' = Vhat Q (so K U' = C', C' orthonormal). Output rows:
+// [U_old (kc) | C_old (kc) | Krylov slots kc..m], columns [U' (k) | C' (k)],
+// with the storage scales d (U) and sigma (slots) folded in.
+static bool recycle_coefficients(int m, int k, const double* hb, std::vector<double2>& coef,
+                                 int& src_kc) {
+    using dense::cd;
+    const int L = int(hb[hb_tail(m, k)]), kc = int(hb[hb_tail(m, k) + 1]);
+    src_kc = kc;
+    if (L - kc < 1 || L < k || L > m || kc > k) return false;
+    const double* graw = hb + hb_graw(m);
+    const double* bd = hb + hb_bd(m);
+    const double* sigma = hb + hb_sigma(m, k);
+    const double* d = hb + hb_d(m, k);
+    const int r = L + 1;
+    std::vector<cd> G(size_t(r) * L, cd(0.0)), W(size_t(r) * L, cd(0.0));
+    for (int t = 0; t < L; ++t) {
+        if (t < kc) {
+            G[t + size_t(r) * t] = d[t];
+            for (int sl = 0; sl < r; ++sl) {
+                const double* v = bd + 2 * (sl + (m + 1) * t);
+                W[sl + size_t(r) * t] = cd(v[0], v[1]);
+            }
+        } else {
+            for (int sl = 0; sl <= t + 1; ++sl) {
+                const double* v = graw + 2 * (t * (m + 1) + sl);
+                G[sl + size_t(r) * t] = cd(v[0], v[1]);
+            }
+            W[t + size_t(r) * t] = 1.0;
+        }
+    }
+    std::vector<cd> P, theta;
+    if (!dense::harmonic_ritz(L, k, G, W, P, theta)) return false;
+    std::vector<cd> GP(size_t(r) * k, cd(0.0)), Q, Rq;
+    for (int c = 0; c < k; ++c)
+        for (int t = 0; t < L; ++t) {
+            const cd pv = P[t + size_t(L) * c];
+            for (int sl = 0; sl < r; ++sl) GP[sl + size_t(r) * c] += G[sl + size_t(r) * t] * pv;
+        }
+    if (!dense::qr(r, k, GP, Q, Rq)) return false;
+    std::vector<cd> Pu(size_t(L) * k);  // P Rq^{-1}
+    for (int t = 0; t < L; ++t)
+        for (int c = 0; c < k; ++c) {
+            cd acc = P[t + size_t(L) * c];
+            for (int q = 0; q < c; ++q) acc -= Pu[t + size_t(L) * q] * Rq[q + size_t(k) * c];
+            Pu[t + size_t(L) * c] = acc / Rq[c + size_t(k) * c];
+        }
+    const int rows = kc + m + 1;
+    coef.assign(size_t(rows) * 2 * k, make_double2(0.0, 0.0));
+    bool finite = true;
+    auto put = [&](int row, int col, cd v) {
+        finite = finite && std::isfinite(v.real()) && std::isfinite(v.imag());
+        coef[size_t(row) * 2 * k + col] = make_double2(v.real(), v.imag());
+    };
+    for (int c = 0; c < k; ++c) {
+        for (int t = 0; t < L; ++t) {
+            const cd v = Pu[t + size_t(L) * c];
+            if (t < kc) put(t, c, v * d[t]);
+            else put(kc + t, c, v * sigma[t]);
+        }
+        for (int sl = 0; sl < r; ++sl) {
+            const cd v = Q[sl + size_t(r) * c];
+            put(kc + sl, k + c, sl < kc ? v : v * sigma[sl]);
+        }
+    }
+    return finite;
+}
 
 template <typename R, typename S, bool ADJ>
 static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_params& p,
@@ -812,21 +1235,55 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     if (lsq_smem > 48 * 1024)
         USV_CUDA_TRY(cudaFuncSetAttribute(k_lsq, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(lsq_smem)));
+    const int kr = g.kr;
+    dim3 grid_bd, grid_comb;
+    size_t bd_smem = 0, comb_smem = 0;
+    if (kr > 0) {
+        using T = typename Wide<S>::T;
+        bd_smem = sizeof(T) * size_t(kr) * kBdTile + sizeof(double2) * size_t(g.m + 1) * kr;
+        comb_smem = sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
+        USV_CUDA_TRY(cudaFuncSetAttribute(k_bdots<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(bd_smem)));
+        USV_CUDA_TRY(cudaFuncSetAttribute(k_combine<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(comb_smem)));
+        if (int e = grid_for((const void*)k_bdots<S>, kThreads, bd_smem, grid_bd)) return e;
+        if (int e = grid_for((const void*)k_combine<S>, kThreads, comb_smem, grid_comb)) return e;
+    }
     // zero the state and the solution
     USV_CUDA_TRY(cudaMemsetAsync(ws + L.state_begin, 0, L.total - L.state_begin, strm));
-    // paired loads may touch the padding past node n-1 of each basis vector:
-    // keep it zero so it contributes nothing to the dots
-    if (g.nv > g.n)
+    if (kr > 0) {
+        // Krylov and pair buffers start zero: every load stays finite, padding included
+        USV_CUDA_TRY(cudaMemsetAsync(ws + L.V, 0, L.coef - L.V, strm));
+    } else if (g.nv > g.n) {
+        // paired loads may touch the padding past node n-1 of each basis vector:
+        // keep it zero so it contributes nothing to the dots
         USV_CUDA_TRY(cudaMemset2DAsync(V + g.n, g.nv * sizeof(C2), 0, (g.nv - g.n) * sizeof(C2),
                                        size_t(g.m + 1) * B, strm));
+    }
     USV_CUDA_TRY(cudaMemset2DAsync(x, ld * sizeof(double2), 0, g.n * sizeof(double2), B, strm));
-    k_residual<ADJ, C2><<<grid_res, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
-    USV_CUDA_TRY(cudaGetLastError());
+    if (kr == 0) {
+        k_residual<ADJ, C2><<<grid_res, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
+        USV_CUDA_TRY(cudaGetLastError());
+    }
+    // Recycling: pinned host blocks for the per-cycle read of the Hessenberg /
+    // inner-product data and the upload of the control words and coefficients.
+    struct Pinned {
+        void* p = nullptr;
+        ~Pinned() { if (p) cudaFreeHost(p); }
+    } hb_pin, up_pin[2];
+    const size_t hb_bytes = sizeof(double) * size_t(B) * (kr > 0 ? g.hb_len : 0);
+    const size_t coef_elems = size_t(kr + g.m + 1) * 2 * kr;
+    const size_t up_ctl_bytes = sizeof(int) * size_t(B) * kCtl;
+    const size_t up_bytes = up_ctl_bytes + sizeof(double2) * coef_elems * B;
+    if (kr > 0) {
+        USV_CUDA_TRY(cudaMallocHost(&hb_pin.p, hb_bytes));
+        for (auto& u : up_pin) USV_CUDA_TRY(cudaMallocHost(&u.p, up_bytes));
+    }
 
     // Event timing: one event before the first kernel of a cycle and one after
     // every kernel; consecutive pairs bracket single launches.
     usv_gmres_profile* prof = p.profile;
-    const int kernels_per_cycle = 2 * g.m + 3;
+    const int kernels_per_cycle = 2 * g.m + 3 + (kr > 0 ? 3 : 0);
     std::vector<cudaEvent_t> ev;
     std::vector<int> fam;
     if (prof) {
@@ -845,13 +1302,31 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         fam.clear();
         fam_bytes.clear();
         USV_CUDA_TRY(mark(st, k++, capturing));
+        if (kr > 0) {
+            // new pair (when the host supplied coefficients), FP64 residual into
+            // slot kc, projection of it on the recycled C
+            k_combine<S><<<grid_comb, kThreads, comb_smem, st>>>(V, g.n, g);
+            USV_CUDA_TRY(mark(st, k++, capturing));
+            fam.push_back(6);
+            fam_bytes.push_back(nn * vb * (2.0 * g.m + 2 * kr + 1));
+            k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
+            USV_CUDA_TRY(mark(st, k++, capturing));
+            fam.push_back(4);
+            fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
+            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, 0, step_d, 1);
+            k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, 0, 1);
+            USV_CUDA_TRY(mark(st, k++, capturing));
+            fam.push_back(6);
+            fam_bytes.push_back(nn * vb * (2.0 * kr + 3));
+        }
         for (int j = 0; j < g.m; ++j) {
-            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d);
+            k_dots<R, S, ADJ, kDotsThreads>
+                <<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
             // read u_0..u_j (u_j also feeds the stencil) + node record, write w
             fam_bytes.push_back(nn * (vb * (j + 2) + 4.0 * sizeof(R)));
-            k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j);
+            k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(1);
             fam_bytes.push_back(nn * vb * (j + 3));
@@ -864,10 +1339,19 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(3);
         fam_bytes.push_back(nn * (vb * g.m + 2 * sizeof(double2) + sizeof(double4)));
-        k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
-        USV_CUDA_TRY(mark(st, k++, capturing));
-        fam.push_back(4);
-        fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
+        if (kr > 0) {
+            // inner products for the harmonic Ritz step, then the host-read block
+            k_bdots<S><<<grid_bd, kThreads, bd_smem, st>>>(V, g.n, g);
+            USV_CUDA_TRY(mark(st, k++, capturing));
+            fam.push_back(6);
+            fam_bytes.push_back(nn * vb * (g.m + 1.0 + kr));
+            USV_CUDA_TRY(cudaMemcpyAsync(hb_pin.p, ws + L.hb, hb_bytes, cudaMemcpyDeviceToHost, st));
+        } else {
+            k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
+            USV_CUDA_TRY(mark(st, k++, capturing));
+            fam.push_back(4);
+            fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
+        }
         USV_CUDA_TRY(cudaGetLastError());
         return USV_OK;
     };
@@ -899,6 +1383,15 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     int rc = USV_OK;
     bool pending = false;
     const int max_cycles = p.maxiter + 2;  // safety bound; the device status ends the loop
+    // Recycling bookkeeping per RHS (lagged by one cycle): the pair, recycled
+    // count and Krylov buffer of the last two launched cycles, and the
+    // coefficients computed from the older one while the newer one runs.
+    struct CycleUse { int pair = -1, kc = 0, vbuf = 0; };
+    struct Pending { bool ready = false; int src_kc = 0; std::vector<double2> coef; };
+    std::vector<CycleUse> last(B), before(B);
+    std::vector<Pending> pend(B);
+    std::vector<double> hb_cur(kr > 0 ? hb_bytes / sizeof(double) : 0);
+    const int every = p.recycle_every > 0 ? p.recycle_every : 1;
     for (int cycle = 0; cycle <= max_cycles; ++cycle) {
         cudaError_t e = cudaMemcpyAsync(status.data(), ws + L.status, sizeof(int) * B,
                                         cudaMemcpyDeviceToHost, strm);
@@ -913,6 +1406,53 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         for (int b = 0; b < B; ++b) any += status[b] == ST_ACTIVE;
         if (!any) break;
         active[0] = any;
+        if (kr > 0) {
+            if (cycle > 0) std::memcpy(hb_cur.data(), hb_pin.p, hb_bytes);
+            // control words of this cycle
+            int* ctl = static_cast<int*>(up_pin[cycle & 1].p);
+            double2* coef = reinterpret_cast<double2*>(static_cast<char*>(up_pin[cycle & 1].p) +
+                                                       up_ctl_bytes);
+            bool any_combine = false;
+            std::vector<CycleUse> now(B);
+            for (int b = 0; b < B; ++b) {
+                int* cw = ctl + b * kCtl;
+                CycleUse u;
+                u.vbuf = cycle % kVBufs;
+                if (pend[b].ready && before[b].vbuf == u.vbuf) {
+                    int dst = 0;
+                    while (dst == before[b].pair || dst == last[b].pair) ++dst;
+                    cw[CW_KC] = kr;
+                    cw[CW_PAIR] = dst;
+                    cw[CW_COMBINE] = 1;
+                    cw[CW_SRC_PAIR] = before[b].pair;
+                    cw[CW_SRC_VBUF] = before[b].vbuf;
+                    cw[CW_SRC_KC] = pend[b].src_kc;
+                    cw[CW_DST] = dst;
+                    std::memcpy(coef + coef_elems * b, pend[b].coef.data(),
+                                sizeof(double2) * pend[b].coef.size());
+                    u.pair = dst;
+                    u.kc = kr;
+                    any_combine = true;
+                } else {
+                    cw[CW_KC] = last[b].kc;
+                    cw[CW_PAIR] = last[b].pair > 0 ? last[b].pair : 0;
+                    cw[CW_COMBINE] = 0;
+                    cw[CW_SRC_PAIR] = cw[CW_SRC_VBUF] = cw[CW_SRC_KC] = cw[CW_DST] = 0;
+                    u.pair = last[b].pair;
+                    u.kc = last[b].kc;
+                }
+                cw[CW_VBUF] = u.vbuf;
+                pend[b].ready = false;
+                now[b] = u;
+            }
+            e = cudaMemcpyAsync(ws + L.ctl, ctl, up_ctl_bytes, cudaMemcpyHostToDevice, strm);
+            if (e == cudaSuccess && any_combine)
+                e = cudaMemcpyAsync(ws + L.coef, coef, sizeof(double2) * coef_elems * B,
+                                    cudaMemcpyHostToDevice, strm);
+            if (e != cudaSuccess) { rc = set_last_cuda_error(e); break; }
+            before = last;
+            last = now;
+        }
         if (exec) {
             e = cudaGraphLaunch(exec, strm);
             if (e != cudaSuccess) { rc = set_last_cuda_error(e); break; }
@@ -921,6 +1461,14 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             if (rc) break;
         }
         pending = true;
+        if (kr > 0 && cycle > 0 && (cycle - 1) % every == 0) {
+            // harmonic Ritz step on the previous cycle's data while this one runs
+            for (int b = 0; b < B; ++b)
+                if (status[b] == ST_ACTIVE)
+                    pend[b].ready = recycle_coefficients(g.m, kr, hb_cur.data() + size_t(b) * g.hb_len,
+                                                         pend[b].coef, pend[b].src_kc) &&
+                                    pend[b].src_kc == before[b].kc;
+        }
     }
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -992,6 +1540,8 @@ static int check_params(const usv_scene* scene, const usv_gmres_params* p, int n
         p->precision != USV_PREC_MIXED_BF16)
         return USV_ERR_ARG;
     *m = int(p->restart < *n ? p->restart : *n);
+    if (p->recycle < 0 || p->recycle_every < 0) return USV_ERR_ARG;
+    if (p->recycle > 0 && (p->recycle > kMaxRecycle || p->recycle > *m - 1)) return USV_ERR_ARG;
     *chunk = kChunk;  // node chunk per CTA (block_nodes is reserved)
     if (p->block_nodes != 0 && p->block_nodes != kChunk) return USV_ERR_ARG;
     *nblk = int((*n + *chunk - 1) / *chunk);
@@ -1012,7 +1562,7 @@ int usv_gmres_workspace_bytes(const usv_scene* scene, const usv_gmres_params* pa
     if (st) return st;
     if (!bytes) return USV_ERR_ARG;
     const size_t vb = vector_bytes(params->precision);
-    *bytes = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity).total;
+    *bytes = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity, params->recycle).total;
     return USV_OK;
 }
 
@@ -1025,7 +1575,8 @@ int usv_gmres_solve(const usv_scene* scene, const void* op_buf, const usv_gmres_
     if (st) return st;
     if (!op_buf || !rhs || !x || !workspace || !stats || ld < n) return USV_ERR_ARG;
     const size_t vb = vector_bytes(params->precision);
-    const WsLayout L = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity);
+    const int kr = params->recycle;
+    const WsLayout L = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity, kr);
     if (workspace_bytes < L.total) return USV_ERR_WORKSPACE;
     char* ws = static_cast<char*>(workspace);
     GState g{};
@@ -1057,6 +1608,22 @@ int usv_gmres_solve(const usv_scene* scene, const void* op_buf, const usv_gmres_
     g.len = reinterpret_cast<int*>(ws + L.len);
     g.ended = reinterpret_cast<int*>(ws + L.ended);
     g.counter = reinterpret_cast<unsigned*>(ws + L.counter);
+    g.ps = partial_slots(m, kr);
+    g.kr = kr;
+    if (kr > 0) {
+        g.hb_len = hb_size(m, kr);
+        g.vstride = (long long)nrhs * (m + 1) * g.nv;
+        g.pstride = (long long)nrhs * kr * g.nv;
+        g.Ubuf = ws + L.U;
+        g.Cbuf = ws + L.C;
+        g.ctl = reinterpret_cast<int*>(ws + L.ctl);
+        g.coef = reinterpret_cast<double2*>(ws + L.coef);
+        g.hb = reinterpret_cast<double*>(ws + L.hb);
+        g.dU = reinterpret_cast<double*>(ws + L.dU);
+        g.alpha = reinterpret_cast<double2*>(ws + L.alpha);
+        g.klast = reinterpret_cast<int*>(ws + L.klast);
+        g.started = reinterpret_cast<int*>(ws + L.started);
+    }
     cudaStream_t strm = static_cast<cudaStream_t>(stream);
     const double2* b = static_cast<const double2*>(rhs);
     double2* xx = static_cast<double2*>(x);

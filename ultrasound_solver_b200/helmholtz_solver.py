@@ -75,6 +75,8 @@ class HelmholtzB200Solver:
             full_cycles=bool(s.get("gmres_full_cycles", True)),
             use_graph=bool(s.get("cuda_graph", True)),
             block_nodes=int(s.get("block_nodes", 0)),
+            recycle=int(s.get("gmres_recycle", 0)),
+            recycle_every=int(s.get("gmres_recycle_every", 1)),
         )
 
     # ----------------------------------------------------------- scene

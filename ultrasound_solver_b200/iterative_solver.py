@@ -14,6 +14,13 @@ Krylov vectors stored as bfloat16 complex (4 bytes per node; the fp32
 stencil and FP64 dots widen them on load), which halves the basis traffic;
 the FP64 refinement at every restart keeps the converged solution the same.
 precision="fp64": complex128 throughout — the plain FP64 comparator.
+
+recycle=k > 0 turns each restart into a GCRO-DR(m, k) cycle (Parks et al.
+2006): k harmonic Ritz vectors of the previous cycles are kept as a pair
+(U, C = K U), every new residual is projected on C first and the Arnoldi
+process runs m - k steps orthogonal to C. The host computes the harmonic Ritz
+step of one cycle while the next runs (one cycle of lag). recycle=0 (the
+default) is the reference's plain restarted GMRES.
 """
 from __future__ import annotations
 
@@ -34,7 +41,8 @@ class B200IterativeSolver:
     def __init__(self, restart: int = 30, maxiter: int = 3000, rtol: float = 1.0e-6,
                  backward_error_tol: float = 1.0e-4, precision: str = "mixed",
                  full_cycles: bool = True, use_graph: bool = True, block_nodes: int = 0,
-                 verbose: bool = False, profile: bool = False):
+                 verbose: bool = False, profile: bool = False, recycle: int = 0,
+                 recycle_every: int = 1):
         if str(precision).lower() not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         self.restart = int(restart)
@@ -45,6 +53,8 @@ class B200IterativeSolver:
         self.full_cycles = bool(full_cycles)
         self.use_graph = bool(use_graph)
         self.block_nodes = int(block_nodes)
+        self.recycle = int(recycle)
+        self.recycle_every = int(recycle_every)
         self.verbose = bool(verbose)
         self.profile = bool(profile)
         self.last_profile = None
@@ -55,7 +65,7 @@ class B200IterativeSolver:
         self.last_history = []
 
     def history_capacity(self) -> int:
-        return self.maxiter // max(self.restart, 1) + 2
+        return self.maxiter // max(self.restart - max(self.recycle, 0), 1) + 2
 
     def params(self, adjoint: bool = False) -> N.GmresParams:
         p = N.GmresParams()
@@ -67,6 +77,8 @@ class B200IterativeSolver:
         p.use_graph = 1 if self.use_graph else 0
         p.block_nodes = self.block_nodes
         p.history_capacity = self.history_capacity()
+        p.recycle = self.recycle
+        p.recycle_every = self.recycle_every
         return p
 
     def workspace_bytes(self, operator, nrhs: int, adjoint: bool = False) -> int:
