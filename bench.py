@@ -1,20 +1,23 @@
 #!/usr/bin/env python
 """RHS solves/s of the gpu_iterative Helmholtz path on B200.
 
-Workload (one "step" = one right-hand side solved to the scaled relative
-residual rtol): the 128^3 variable-medium scene at h = 1 mm, 40 kHz, seeded
-Gaussian random c and rho (sigma = 4 cells, +-3 clip), a rho=1250/c=2200
-blended sphere of radius 15 mm 60 mm above the baffle, +x reflecting wall,
-10-cell quadratic PML on the other open faces, 8 x 8 sinc_neumann array
-(radius 4.5 mm, pitch 10.5 mm), seeded phases. Inputs are synthetic.
+Workload (one "step" = one batch of `--batch` right-hand sides, each solved to
+the scaled relative residual rtol): the 128^3 variable-medium scene at
+h = 1 mm, 40 kHz, seeded Gaussian random c and rho (sigma = 4 cells, +-3
+clip), a rho=1250/c=2200 blended sphere of radius 15 mm 60 mm above the
+baffle, +x reflecting wall, 10-cell quadratic PML on the other open faces,
+8 x 8 sinc_neumann array (radius 4.5 mm, pitch 10.5 mm), seeded phases (one
+phase vector per right-hand side). Inputs are synthetic.
 
-Our arm: mixed-precision GMRES (complex64 Krylov vectors, FP64 dots,
-Hessenberg/Givens, true residual and solution update at every restart) on
-the matrix-free sm_100a stencil; the plain FP64 GMRES of the same stencil is
-timed once beside it, and the relative L2 difference between the two
-solutions is reported. `--impl reference` times the reference's CPU
-algorithm (the oracle's restatement: CSR assembly + row-scaled Jacobi GMRES
-in scipy/numpy) on the host cores.
+Our arm: mixed-precision batched solves on the matrix-free sm_100a stencil:
+bfloat16 Krylov vectors (fp32 stencil, FP64 dots, Hessenberg/Givens, FP64
+true residual and solution update at every restart) with deflated restarting
+(GCRO-DR(40, 10): 10 harmonic Ritz vectors recycled across restarts). The
+plain FP64 GMRES(30) of the same stencil (the reference's algorithm in FP64)
+is timed once beside it on the first right-hand side, and the relative L2
+difference between the two solutions is reported. `--impl reference` times
+the reference's CPU algorithm (the oracle's restatement: CSR assembly +
+row-scaled Jacobi GMRES(30) in scipy/numpy) on the host cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -36,12 +39,15 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "RHS solves/s at 128^3 (config-1 scene), mixed-precision GMRES, rel err <=1e-6 vs FP64"
+# the reference's algorithm: row-scaled Jacobi GMRES(30)
+REFERENCE_RESTART = 30
 UNIT = "RHS solves/s"
 FALLBACK_HBM_GBS = 6650.0
-# Inner iterations the row-scaled Jacobi GMRES(112) needs on this scene to
-# reach rtol 1e-9 (FP64 arm of this bench on a B200); the CPU sample below is
-# converted to solves/s with it because a full CPU solve takes hours.
-ITERATIONS_PER_SOLVE_FP64 = 32816
+# Inner iterations the row-scaled Jacobi GMRES(30) needs on this scene to
+# reach rtol 1e-9 (FP64 GMRES(30) of this bench on a B200); the CPU sample is
+# converted to solves/s with it (or with the FP64 arm's count of the same
+# run) because a full CPU solve takes hours.
+ITERATIONS_PER_SOLVE_FP64 = 52950
 # DRAM bytes / algorithmic bytes of the Arnoldi kernels from one ncu capture
 # (profiles/arnoldi_kdots_korth_128cube_m112_j56.md); the roofline's `traffic`
 # is the algorithmic bytes per launch scaled by it.
@@ -55,9 +61,15 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--grid", type=int, default=128)
-    ap.add_argument("--restart", type=int, default=112)
+    ap.add_argument("--restart", type=int, default=40)
+    ap.add_argument("--recycle", type=int, default=10,
+                    help="harmonic Ritz vectors recycled across restarts (0: plain GMRES)")
+    ap.add_argument("--recycle-every", type=int, default=2)
+    ap.add_argument("--precision", default="bf16", choices=("bf16", "mixed"))
+    ap.add_argument("--batch", type=int, default=4, help="right-hand sides per step")
+    ap.add_argument("--fp64-restart", type=int, default=REFERENCE_RESTART)
     ap.add_argument("--rtol", type=float, default=1e-9)
-    ap.add_argument("--maxiter", type=int, default=60000)
+    ap.add_argument("--maxiter", type=int, default=80000)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GMRES comparator")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -171,14 +183,22 @@ def max_over_ranks(value, world):
 def workload_config(args):
     from ultrasound_solver_b200 import workloads as W
     cfg = W.config1(n=args.grid)
+    vb = 4 if args.precision == "bf16" else 8
     desc = {"workload": f"config-1 scene: {args.grid}^3 nodes h=1mm 40kHz, random c/rho "
                         "(sigma 4 cells), r=15mm rho=1250 sphere blended, +x reflecting, "
-                        "10-cell quadratic PML, 8x8 sinc_neumann array, 1 RHS per step",
-            "grid": [args.grid] * 3, "nodes": args.grid ** 3, "restart": args.restart,
-            "rtol": args.rtol, "precision": "complex64 Krylov + FP64 refinement",
-            "l2": "inputs larger than L2 (Krylov basis %.1f GB)" % (
-                (args.restart + 1) * args.grid ** 3 * 8 / 1e9),
-            "parallelism": "replicas (independent RHS per GPU)"}
+                        f"10-cell quadratic PML, 8x8 sinc_neumann array, {args.batch} RHS "
+                        "(seeded phase vectors) per step",
+            "grid": [args.grid] * 3, "nodes": args.grid ** 3, "rhs_per_step": args.batch,
+            "solver": (f"GCRO-DR({args.restart},{args.recycle}) deflated restarting, "
+                       f"recycled space refreshed every {args.recycle_every} cycles"
+                       if args.recycle else f"GMRES({args.restart})"),
+            "restart": args.restart, "recycle": args.recycle, "rtol": args.rtol,
+            "precision": ("bfloat16" if args.precision == "bf16" else "complex64")
+                         + " Krylov vectors, FP64 dots/Hessenberg + FP64 refinement",
+            "fp64_comparator": f"plain FP64 GMRES({args.fp64_restart}), 1 RHS",
+            "l2": "inputs larger than L2 (Krylov basis %.1f GB per RHS)" % (
+                2 * (args.restart + 1) * args.grid ** 3 * vb / 1e9),
+            "parallelism": "replicas (independent RHS batches per GPU)"}
     return cfg, desc
 
 
@@ -191,21 +211,31 @@ def run_ours(args):
     cfg, desc = workload_config(args)
     solver = W.build_solver(cfg, seed=0)
     rng = np.random.default_rng(1 + rank)
-    solver.set_phases(rng.uniform(0, 2 * np.pi, solver.transducers.num_transducers))
     solver.assemble_matrix()
-    rhs = solver.update_rhs_device()
+    rhs_list = []
+    for _ in range(args.batch):
+        solver.set_phases(rng.uniform(0, 2 * np.pi, solver.transducers.num_transducers))
+        rhs_list.append(solver.update_rhs_device())
+    rhs = torch.stack(rhs_list)
     it = solver.iterative_solver
-    it.restart, it.rtol, it.maxiter = args.restart, args.rtol, args.maxiter
+    it.rtol, it.maxiter = args.rtol, args.maxiter
     it.backward_error_tol = 1e-4
     stream = torch.cuda.current_stream()
 
-    def solve(precision, profile=False):
+    def configure(precision, profile=False):
         it.precision, it.profile = precision, profile
-        return it.solve(solver.operator, rhs)
+        if precision == "fp64":
+            it.restart, it.recycle = args.fp64_restart, 0
+        else:
+            it.restart, it.recycle, it.recycle_every = args.restart, args.recycle, args.recycle_every
+
+    def solve(precision, profile=False, b=None):
+        configure(precision, profile)
+        return it.solve(solver.operator, rhs if b is None else b)
 
     # warm-up (untimed)
     for _ in range(args.warmup):
-        x_mixed = solve("mixed")
+        x_mixed = solve(args.precision)
     torch.cuda.synchronize()
     # timed region: K solves from device-resident inputs
     barrier(world)
@@ -218,25 +248,29 @@ def run_ours(args):
         stop = torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for _ in range(args.steps):
-            x_mixed = solve("mixed", profile=True)
+            x_mixed = solve(args.precision, profile=True)
             iterations.append(it.last_iterations)
             for name, d in it.last_profile.items():
                 agg = prof_tot.setdefault(name, dict(launches=0, ms=0.0, bytes=0.0))
                 for k in agg:
                     agg[k] += d[k]
-            launches += sum(d["launches"] for d in it.last_profile.values()) + 1
+            # measured intervals + the second kernel of each projection interval
+            # (one per recycled cycle: half of the recycle_dots intervals)
+            launches += sum(d["launches"] for d in it.last_profile.values())
+            launches += it.last_profile.get("recycle_dots", {}).get("launches", 0) // 2
         stop.record(stream)
         torch.cuda.synchronize()
     barrier(world)
     ms_local = start.elapsed_time(stop)
     ms = max_over_ranks(ms_local, world)
-    value = world * args.steps / (ms / 1000.0)
+    value = world * args.steps * args.batch / (ms / 1000.0)
     stats = dict(it.last_stats[0])
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "c64+f64", "data": "synthetic", "config": desc,
+           "dtype": ("bf16" if args.precision == "bf16" else "c64") + "+f64",
+           "data": "synthetic", "config": desc,
            "iterations_per_solve": iterations, "scaled_residual": stats["scaled_residual"],
            "backward_error": stats["backward_error"]}
     out["clocks"] = clocks.summary()
@@ -261,34 +295,36 @@ def run_ours(args):
                                     for k, v in prof_tot.items()}}
 
     # plain FP64 GMRES of the same stencil (comparator) + parity of the two fields
+    fp64_iters = None
     if not args.no_fp64:
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        x64 = solve("fp64")
+        x64 = solve("fp64", b=rhs[0])
         e1.record(stream)
         torch.cuda.synchronize()
         ms64 = e0.elapsed_time(e1)
-        rel = float((torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item())
+        fp64_iters = it.last_iterations
+        rel = float((torch.linalg.norm(x_mixed[0] - x64) / torch.linalg.norm(x64)).item())
         out["fp64_gmres"] = {"solves_per_s": 1000.0 / ms64, "ms_per_solve": ms64,
-                             "iterations": it.last_iterations,
+                             "iterations": fp64_iters, "restart": args.fp64_restart,
                              "speedup_mixed_vs_fp64": (value / world) / (1000.0 / ms64)}
         out["rel_err_vs_fp64"] = rel
 
     # end to end through the public API with host buffers
     if not args.no_e2e:
-        it.precision, it.profile = "mixed", False
-        rhs_host = rhs.cpu().numpy()
+        configure(args.precision)
+        rhs_host = np.ascontiguousarray(rhs.cpu().numpy().T)  # (N, B), the reference's layout
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        n_e2e = max(1, min(args.steps, 2))
+        n_e2e = 1
         for _ in range(n_e2e):
             xh = solver.solve_rhs(rhs_host, verbose=False)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         e2e = max_over_ranks(dt, world)
-        out["e2e"] = {"value": world * n_e2e / e2e, "unit": UNIT,
+        out["e2e"] = {"value": world * n_e2e * args.batch / e2e, "unit": UNIT,
                       "h2d_bytes_per_step": int(rhs_host.nbytes),
                       "d2h_bytes_per_step": int(xh.nbytes), "steps": n_e2e,
                       "api": "HelmholtzB200Solver.solve_rhs(numpy)"}
@@ -297,7 +333,7 @@ def run_ours(args):
     if not args.no_adjoint:
         from ultrasound_solver_b200.autograd import loss_of_field, phase_field
         from ultrasound_solver_b200.losses import ContrastRatioLoss
-        it.precision, it.profile = "mixed", False
+        configure(args.precision)
         centre = (args.grid - 1) * solver.cfg.domain.dx / 2
         loss = ContrastRatioLoss(solver.cfg, (centre, centre, 0.080), 0.006, 0.010)
         ph = torch.tensor(solver.transducers.phases, dtype=torch.float64, device="cuda",
@@ -317,7 +353,7 @@ def run_ours(args):
                                "grad_norm": float(torch.linalg.norm(ph.grad).item())}
 
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_sample(args, cfg)
+        out["cpu_baseline"] = cpu_sample(args, cfg, fp64_iters)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -350,7 +386,7 @@ def cpu_iterations_per_second(args, sc, iters):
     A = sc.A
     R, inv_d = O.row_scale_and_jacobi(A)
     b = R * sc.rhs
-    m = min(args.restart, iters)
+    m = min(args.fp64_restart, iters)
     t0 = time.perf_counter()
     # one truncated cycle of the restated algorithm: m steps of CGS Arnoldi
     r = b.copy()
@@ -375,15 +411,17 @@ def blas_threads():
         return 1
 
 
-def cpu_sample(args, cfg):
+def cpu_sample(args, cfg, fp64_iters=None):
     sc = cpu_scene(args, cfg)
     its, m, dt = cpu_iterations_per_second(args, sc, args.cpu_iters)
-    return {"value": its / ITERATIONS_PER_SOLVE_FP64, "unit": UNIT, "cores": blas_threads(),
+    per_solve = fp64_iters or ITERATIONS_PER_SOLVE_FP64
+    return {"value": its / per_solve, "unit": UNIT, "cores": blas_threads(),
             "kind": "port",
-            "sample": (f"{m} Arnoldi steps of the restated row-scaled Jacobi GMRES({args.restart}) "
-                       f"on the {args.grid}^3 scene in {dt:.1f}s ({its:.2f} it/s, scipy CSR SpMV "
-                       f"single-threaded); solves/s = it/s / {ITERATIONS_PER_SOLVE_FP64} "
-                       "iterations per solve")}
+            "sample": (f"{m} Arnoldi steps of the restated row-scaled Jacobi "
+                       f"GMRES({args.fp64_restart}) on the {args.grid}^3 scene in {dt:.1f}s "
+                       f"({its:.2f} it/s, scipy CSR SpMV single-threaded); solves/s = it/s / "
+                       f"{per_solve} iterations per solve (GMRES({args.fp64_restart}) to "
+                       f"rtol {args.rtol:g} on this scene)")}
 
 
 def run_reference(args):
@@ -409,7 +447,7 @@ def run_reference(args):
            "data": "synthetic", "config": desc, "impl": "reference",
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": (f"{args.cpu_iters} Arnoldi steps per step of the restated "
-                                       f"row-scaled Jacobi GMRES({args.restart}) (reference CPU "
+                                       f"row-scaled Jacobi GMRES({args.fp64_restart}) (reference CPU "
                                        f"algorithm, CuPy gmres restated in numpy/scipy); "
                                        f"{its:.3f} it/s; solves/s = it/s / "
                                        f"{ITERATIONS_PER_SOLVE_FP64} iterations per solve")},

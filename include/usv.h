@@ -101,9 +101,9 @@ typedef struct usv_scene {
  * recorded between the launches (also inside the captured cycle graph).
  * Families: 0 Arnoldi stencil+dots, 1 orthogonalisation+norm,
  * 2 least squares, 3 solution update, 4 FP64 residual, 5 final gates,
- * 6 recycled-space kernels (new pair, projection, harmonic Ritz dots),
- * 7 unused. `launches` counts measured intervals (a projection interval
- * holds two kernels). */
+ * 6 new recycled pair, 7 projection on the recycled space and the inner
+ * products of the harmonic Ritz step. `launches` counts measured intervals
+ * (a projection interval holds two kernels). */
 #define USV_KFAMILIES 8
 typedef struct usv_gmres_profile {
     int32_t launches[USV_KFAMILIES];
@@ -142,6 +142,13 @@ typedef struct usv_gmres_stats {
     double backward_error;       /* max |Ax-b| / (|A||x|+|b|), fp64              */
     double initial_residual;     /* ||Rb||                                       */
 } usv_gmres_stats;
+
+/* Host-only (no GPU work): the harmonic Ritz step of the recycled cycles.
+ * G and W are (m+1) x m complex column-major (interleaved re, im): K W_m =
+ * Vhat G and Vhat^H W_m of one cycle. Returns in P (m x k) the k unit
+ * solutions z of G^H G z = theta G^H W z with the smallest |theta|, and the
+ * theta. USV_ERR_NONFINITE when the eigen-solve fails. */
+int usv_harmonic_ritz(int m, int k, const double* G, const double* W, double* P, double* theta);
 
 /* library identity */
 int usv_abi_version(void);

@@ -1,6 +1,7 @@
 """The C ABI library loads and exports every symbol include/usv.h declares (CPU only)."""
 import ctypes
 
+import numpy as np
 import pytest
 
 from ultrasound_solver_b200 import _native, build
@@ -70,3 +71,46 @@ def test_scene_validation_messages():
     s = make_scene((9, 9, 9), 1e-3, 2.5e5, {"+x": {"type": "impedance", "impedance": [400, 1]},
                                              "-y": "soft", "+z": "open"}, {"cells": 2})
     assert list(s.face_kind) == [0, 3, 2, 0, 0, 1] and s.pml_faces == 32
+
+
+def _arnoldi(A, v, m):
+    n = A.shape[0]
+    V = np.zeros((n, m + 1), complex)
+    H = np.zeros((m + 1, m), complex)
+    V[:, 0] = v / np.linalg.norm(v)
+    for j in range(m):
+        w = A @ V[:, j]
+        for _ in range(2):
+            h = V[:, :j + 1].conj().T @ w
+            w -= V[:, :j + 1] @ h
+            H[:j + 1, j] += h
+        H[j + 1, j] = np.linalg.norm(w)
+        V[:, j + 1] = w / H[j + 1, j]
+    return H
+
+
+@pytest.mark.parametrize("m,k,aug", [(30, 10, 0), (40, 10, 4), (60, 16, 8)])
+def test_harmonic_ritz_matches_scipy(lib, m, k, aug):
+    """Host harmonic Ritz step of the recycled cycles against scipy's generalized eig."""
+    import scipy.linalg as sl
+    rng = np.random.default_rng(m)
+    n = 400
+    A = (np.diag(np.linspace(-1, 3, n) + 0.05j)
+         + 0.3 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n))
+    G = _arnoldi(A, rng.standard_normal(n) + 0j, m)
+    W = np.vstack([np.eye(m), np.zeros((1, m))]).astype(complex)
+    if aug:  # leading columns of a recycled cycle: Vhat^H Ut is a general block
+        W[:, :aug] = rng.standard_normal((m + 1, aug)) + 1j * rng.standard_normal((m + 1, aug))
+    Gf, Wf = np.asfortranarray(G), np.asfortranarray(W)
+    P = np.zeros((m, k), complex, order="F")
+    th = np.zeros(k, complex)
+    rc = lib.usv_harmonic_ritz(m, k, Gf.ctypes.data, Wf.ctypes.data, P.ctypes.data, th.ctypes.data)
+    assert rc == 0
+    M1, M2 = G.conj().T @ G, G.conj().T @ W
+    want = np.sort(np.abs(sl.eig(M1, M2, right=False)))[:k]
+    np.testing.assert_allclose(np.sort(np.abs(th)), want, rtol=1e-9)
+    for i in range(k):
+        assert abs(np.linalg.norm(P[:, i]) - 1) < 1e-12
+        assert np.linalg.norm(M1 @ P[:, i] - th[i] * (M2 @ P[:, i])) <= 1e-10 * np.linalg.norm(M1)
+    assert lib.usv_harmonic_ritz(m, m + 1, Gf.ctypes.data, Wf.ctypes.data, P.ctypes.data,
+                                 th.ctypes.data) == 1

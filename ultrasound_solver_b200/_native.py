@@ -41,7 +41,7 @@ class Scene(C.Structure):
 
 KFAMILIES = 8
 KFAMILY_NAMES = ("arnoldi_dots", "arnoldi_orth", "lsq", "update", "residual", "gates",
-                 "recycle", "unused")
+                 "recycle_pair", "recycle_dots")
 
 
 class GmresProfile(C.Structure):
@@ -74,6 +74,7 @@ _SP = C.POINTER(Scene)
 
 _SIGNATURES = {
     "usv_abi_version": ([], _I),
+    "usv_harmonic_ritz": ([_I, _I, _P, _P, _P, _P], _I),
     "usv_status_string": ([_I], C.c_char_p),
     "usv_device_info": ([C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)], _I),
     "usv_operator_bytes": ([_SP, C.POINTER(_SZ)], _I),

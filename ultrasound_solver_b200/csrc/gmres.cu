@@ -479,6 +479,8 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base0, const 
 // all warps work.
 constexpr int kDotUnroll = 8;
 constexpr int kDotsThreads = 512;
+// Dots phase form: warp tasks per vector (k_dots) or streamed per thread (k_dots_stream).
+constexpr bool kStreamDots = true;
 
 template <typename C2> struct LaneLoad;
 template <> struct LaneLoad<bf2> {
@@ -612,6 +614,125 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         for (int sg = 0; sg < segs; ++sg) {
             re += segsum[t * segs + sg].x;
             im += segsum[t * segs + sg].y;
+        }
+        if (t <= j) {
+            const double st = g.sigma[b * (g.m + 1) + t];
+            re *= st;
+            im *= st;
+        }
+        part[t] = make_double2(re, im);
+    }
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    const int nparts = int(gridDim.x);
+    for (int t = warp; t <= j + 1; t += nw) {
+        double re0 = 0.0, im0 = 0.0;
+        const double2* pt = g.partial + (long long)b * g.nblk * g.ps + t;
+        for (int q0 = 0; q0 < nparts; q0 += 32 * 4) {
+            double2 pv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + 32 * u + lane;
+                pv[u] = q < nparts ? ld_cg(pt + (long long)q * g.ps) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                re0 += pv[u].x;
+                im0 += pv[u].y;
+            }
+        }
+        re0 = warp_sum(re0);
+        im0 = warp_sum(im0);
+        if (lane == 0) {
+            if (t > j) g.wnorm[b] = sqrt(re0);
+            else if (proj) g.alpha[(long long)b * g.kr + t] = make_double2(re0, im0);
+            else g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
+        }
+    }
+    if (threadIdx.x == 0) g.counter[b] = 0;
+}
+
+// Arnoldi step j, part 1, streaming form: the same stencil into shared and
+// global memory, then every thread takes the w values of its own node pairs
+// from shared memory and streams u_0..u_j through the cp.async pipeline (the
+// k_orth access pattern); the per-thread products of vector t are reduced
+// across the warp as soon as t is complete and added to a per-warp table in
+// chunk order (deterministic).
+template <typename R, typename S, bool ADJ>
+__global__ void __launch_bounds__(kThreads, 2) k_dots_stream(OpView<R> op, S* V, GState g, int j,
+                                                             Step step, int proj) {
+    using C2 = S;
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    if (proj) {
+        if (cb.kc == 0) return;
+        j = cb.kc - 1;
+    } else if (j < cb.kc) {
+        return;
+    }
+    extern __shared__ __align__(16) uint4 stg[];
+    __shared__ __align__(16) C2 ys[kChunk];
+    constexpr int nw = kThreads / 32;
+    __shared__ double2 tsum[nw][USV_MAX_RESTART + 2];
+    const long long N = op.n;
+    const C2* uj = cb.V + (long long)j * g.nv;
+    C2* w = cb.V + (long long)(j + 1) * g.nv;
+    const R sj = R(g.sigma[b * (g.m + 1) + j]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = threadIdx.x; q < nw * (USV_MAX_RESTART + 2); q += kThreads)
+        (&tsum[0][0])[q] = make_double2(0.0, 0.0);
+    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+        const long long n0 = (long long)ch * kChunk;
+        const int len = int(min((long long)kChunk, N - n0));
+        __syncthreads();  // the previous chunk is done with ys (and tsum is zeroed)
+        if (!proj) {
+            Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
+#pragma unroll 4
+            for (int e = threadIdx.x; e < kChunk; e += kThreads) {
+                C2 y = from_d<C2>(make_double2(0.0, 0.0));
+                if (e < len) {
+                    const long long n = n0 + e;
+                    y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
+                    w[n] = y;
+                }
+                ys[e] = y;
+                advance(p, step, op.nx, op.ny);
+            }
+        } else {
+            for (int e = threadIdx.x; e < kChunk; e += kThreads)
+                ys[e] = e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0));
+        }
+        __syncthreads();
+        double2 y[kPairs][2];
+        double nrm = 0.0;
+#pragma unroll
+        for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                y[k][c] = to_d(ys[pair_node<C2>(k) + c]);
+                nrm += cabs2(y[k][c]);
+            }
+        double pr = 0.0, pi = 0.0;
+        stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
+                         [&](int t, int k, int c, double2 v) {
+            pr = fma(v.x, y[k][c].x, fma(v.y, y[k][c].y, pr));
+            pi = fma(v.x, y[k][c].y, fma(-v.y, y[k][c].x, pi));
+            if (k == kPairs - 1 && c == 1) {  // vector t done for this thread
+                const double re = warp_sum(pr), im = warp_sum(pi);
+                if (lane == 0) tsum[warp][t] = cadd(tsum[warp][t], make_double2(re, im));
+                pr = pi = 0.0;
+            }
+        });
+        nrm = warp_sum(nrm);
+        if (lane == 0) tsum[warp][j + 1].x += nrm;
+    }
+    __syncthreads();
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+    for (int t = threadIdx.x; t <= j + 1; t += kThreads) {
+        double re = 0.0, im = 0.0;
+        for (int q = 0; q < nw; ++q) {
+            re += tsum[q][t].x;
+            im += tsum[q][t].y;
         }
         if (t <= j) {
             const double st = g.sigma[b * (g.m + 1) + t];
@@ -894,14 +1015,15 @@ template <> struct Wide<double2> { using T = double2; };
 // the host-read block. Each CTA stages a tile of U in shared memory; warp w
 // owns the slots s = w (mod warps) for every tile, so the per-CTA sums are
 // accumulated in a fixed order; the last CTA reduces the CTA partials.
-template <typename S>
+template <typename S, int K>
 __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g) {
     using T = typename Wide<S>::T;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
     const CycleBasis<S> cb = cycle_basis(V, g, b);
-    const int kc = cb.kc, m = g.m;
-    if (kc == 0) return;
+    const int m = g.m;
+    if (cb.kc != K) return;  // recycled cycles use all K vectors
+    constexpr int kc = K;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ut = reinterpret_cast<T*>(smem_raw);                                  // [kc][kBdTile]
     double2* tab = reinterpret_cast<double2*>(ut + (size_t)kc * kBdTile);    // [m+1][kc]
@@ -920,26 +1042,25 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
             __syncthreads();
             for (int sl = warp; sl <= m; sl += nw) {
                 const S* vs = (sl < kc ? cb.C : cb.V) + (long long)sl * g.nv + n0;
-                T acc[kMaxRecycle];
+                T acc[K];
 #pragma unroll
-                for (int i = 0; i < kMaxRecycle; ++i) acc[i] = cmake<T>(0.0, 0.0);
+                for (int i = 0; i < K; ++i) acc[i] = cmake<T>(0.0, 0.0);
+#pragma unroll 2
                 for (int e = lane; e < len; e += 32) {
                     const T v = widen<T>(vs[e]);
 #pragma unroll
-                    for (int i = 0; i < kMaxRecycle; ++i)
-                        if (i < kc) {
-                            const T u = ut[i * kBdTile + e];
-                            acc[i].x += v.x * u.x + v.y * u.y;
-                            acc[i].y += v.x * u.y - v.y * u.x;
-                        }
+                    for (int i = 0; i < K; ++i) {
+                        const T u = ut[i * kBdTile + e];
+                        acc[i].x += v.x * u.x + v.y * u.y;
+                        acc[i].y += v.x * u.y - v.y * u.x;
+                    }
                 }
 #pragma unroll
-                for (int i = 0; i < kMaxRecycle; ++i)
-                    if (i < kc) {
-                        const double re = warp_sum(double(acc[i].x));
-                        const double im = warp_sum(double(acc[i].y));
-                        if (lane == 0) tab[sl * kc + i] = cadd(tab[sl * kc + i], make_double2(re, im));
-                    }
+                for (int i = 0; i < K; ++i) {
+                    const double re = warp_sum(double(acc[i].x));
+                    const double im = warp_sum(double(acc[i].y));
+                    if (lane == 0) tab[sl * kc + i] = cadd(tab[sl * kc + i], make_double2(re, im));
+                }
             }
         }
     }
@@ -971,80 +1092,104 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
 // Inputs: the source pair U_0..U_{kc-1}, C_0..C_{kc-1} and the source Krylov
 // slots kc..m; coefficient rows in that order, columns U'_0..U'_{k-1},
 // C'_0..C'_{k-1}. Outputs go to a third pair buffer (no aliasing). Also
-// d'_i = 1/||U'_i|| for the new pair.
-template <typename S>
+// d'_i = 1/||U'_i|| for the new pair. One pass over the inputs: every thread
+// keeps the 2K outputs of kNpt nodes (coalesced, kThreads apart) in
+// registers; the shared coefficient row is read once per kNpt nodes.
+template <typename S> constexpr int kCombineNpt = sizeof(S) == 16 ? 1 : 2;
+template <typename S, int K>
 __global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState g) {
     using T = typename Wide<S>::T;
+    constexpr int NPT = kCombineNpt<S>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE) return;
     const int* cw = g.ctl + b * kCtl;
     if (!cw[CW_COMBINE]) return;
-    const int m = g.m, k = g.kr, skc = cw[CW_SRC_KC];
+    const int m = g.m, skc = cw[CW_SRC_KC];
     const int rows = skc + m + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* cf = reinterpret_cast<T*>(smem_raw);  // [rows][2k]
+    T* cf = reinterpret_cast<T*>(smem_raw);  // [rows][2K]
     __shared__ double sh[32];
-    for (int q = threadIdx.x; q < rows * 2 * k; q += kThreads) {
-        const double2 c = g.coef[(long long)b * (k + m + 1) * 2 * k + q];
+    for (int q = threadIdx.x; q < rows * 2 * K; q += kThreads) {
+        const double2 c = g.coef[(long long)b * (K + m + 1) * 2 * K + q];
         cf[q] = cmake<T>(c.x, c.y);
     }
-    const long long sp = (cw[CW_SRC_PAIR] > 0 ? cw[CW_SRC_PAIR] : 0) * g.pstride + (long long)b * k * g.nv;
-    const long long dp = cw[CW_DST] * g.pstride + (long long)b * k * g.nv;
+    const long long sp = (cw[CW_SRC_PAIR] > 0 ? cw[CW_SRC_PAIR] : 0) * g.pstride + (long long)b * K * g.nv;
+    const long long dp = cw[CW_DST] * g.pstride + (long long)b * K * g.nv;
     const S* Uo = static_cast<const S*>(g.Ubuf) + sp;
     const S* Co = static_cast<const S*>(g.Cbuf) + sp;
     S* Un = static_cast<S*>(g.Ubuf) + dp;
     S* Cn = static_cast<S*>(g.Cbuf) + dp;
     const S* Vs = V + cw[CW_SRC_VBUF] * g.vstride + (long long)b * (m + 1) * g.nv;
     __syncthreads();
-    double nrm[kMaxRecycle];
+    double nrm[K];
 #pragma unroll
-    for (int i = 0; i < kMaxRecycle; ++i) nrm[i] = 0.0;
-    for (long long n = (long long)blockIdx.x * kThreads + threadIdx.x; n < N;
-         n += (long long)gridDim.x * kThreads) {
-        for (int pass = 0; pass < 2; ++pass) {  // 0: U', 1: C'
-            T acc[kMaxRecycle];
+    for (int i = 0; i < K; ++i) nrm[i] = 0.0;
+    auto fma_row = [](T (&acc)[NPT][K], const T* crow, const T (&v)[NPT]) {
 #pragma unroll
-            for (int i = 0; i < kMaxRecycle; ++i) acc[i] = cmake<T>(0.0, 0.0);
-            const int r_end = pass == 0 ? rows - 1 : rows;  // U' does not use slot m
-            for (int r = 0; r < r_end; ++r) {
-                if (pass == 0 && r >= skc && r < 2 * skc) continue;  // C rows feed C' only
-                if (pass == 1 && r < skc) continue;                  // U rows feed U' only
-                const S* src = r < skc ? Uo + (long long)r * g.nv
-                             : r < 2 * skc ? Co + (long long)(r - skc) * g.nv
-                                           : Vs + (long long)(r - skc) * g.nv;
-                const T v = widen<T>(src[n]);
-                const T* crow = cf + r * 2 * k + pass * k;
+        for (int i = 0; i < K; ++i) {
+            const T c = crow[i];
 #pragma unroll
-                for (int i = 0; i < kMaxRecycle; ++i)
-                    if (i < k) {
-                        const T c = crow[i];
-                        acc[i].x += c.x * v.x - c.y * v.y;
-                        acc[i].y += c.x * v.y + c.y * v.x;
-                    }
+            for (int q = 0; q < NPT; ++q) {
+                acc[q][i].x += c.x * v[q].x - c.y * v[q].y;
+                acc[q][i].y += c.x * v[q].y + c.y * v[q].x;
             }
-            S* dst = pass == 0 ? Un : Cn;
+        }
+    };
+    const long long step = (long long)gridDim.x * kThreads * NPT;
+    for (long long n0 = (long long)blockIdx.x * kThreads * NPT + threadIdx.x; n0 < N; n0 += step) {
+        T au[NPT][K], ac[NPT][K];
 #pragma unroll
-            for (int i = 0; i < kMaxRecycle; ++i)
-                if (i < k) {
-                    const S o = narrow<S>(acc[i]);
-                    dst[(long long)i * g.nv + n] = o;
-                    if (pass == 0) nrm[i] += cabs2(to_d(o));
+        for (int q = 0; q < NPT; ++q)
+#pragma unroll
+            for (int i = 0; i < K; ++i) au[q][i] = ac[q][i] = cmake<T>(0.0, 0.0);
+        auto load = [&](const S* src, T (&v)[NPT]) {
+#pragma unroll
+            for (int q = 0; q < NPT; ++q) {
+                const long long n = n0 + (long long)q * kThreads;
+                v[q] = n < N ? widen<T>(src[n]) : cmake<T>(0.0, 0.0);
+            }
+        };
+        T v[NPT];
+        for (int r = 0; r < skc; ++r) {  // U rows feed U' only
+            load(Uo + (long long)r * g.nv, v);
+            fma_row(au, cf + r * 2 * K, v);
+        }
+        for (int r = 0; r < skc; ++r) {  // C rows feed C' only
+            load(Co + (long long)r * g.nv, v);
+            fma_row(ac, cf + (skc + r) * 2 * K + K, v);
+        }
+        for (int sl = skc; sl <= m; ++sl) {  // Krylov slots feed both (slot m: C' only)
+            load(Vs + (long long)sl * g.nv, v);
+            const T* crow = cf + (skc + sl) * 2 * K;
+            if (sl < m) fma_row(au, crow, v);
+            fma_row(ac, crow + K, v);
+        }
+#pragma unroll
+        for (int q = 0; q < NPT; ++q) {
+            const long long n = n0 + (long long)q * kThreads;
+            if (n < N) {
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    const S o = narrow<S>(au[q][i]);
+                    Un[(long long)i * g.nv + n] = o;
+                    Cn[(long long)i * g.nv + n] = narrow<S>(ac[q][i]);
+                    nrm[i] += cabs2(to_d(o));
                 }
+            }
         }
     }
     double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
 #pragma unroll
-    for (int i = 0; i < kMaxRecycle; ++i)
-        if (i < k) {
-            const double t = block_sum(nrm[i], sh);
-            if (threadIdx.x == 0) part[i] = make_double2(t, 0.0);
-        }
+    for (int i = 0; i < K; ++i) {
+        const double t = block_sum(nrm[i], sh);
+        if (threadIdx.x == 0) part[i] = make_double2(t, 0.0);
+    }
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    for (int i = threadIdx.x; i < k; i += kThreads) {
+    for (int i = threadIdx.x; i < K; i += kThreads) {
         double t = 0.0;
         const double2* pq = g.partial + (long long)b * g.nblk * g.ps + i;
         for (int c = 0; c < int(gridDim.x); ++c) t += ld_cg(pq + (long long)c * g.ps).x;
-        g.dU[((long long)cw[CW_DST] * gridDim.y + b) * k + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
+        g.dU[((long long)cw[CW_DST] * gridDim.y + b) * K + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
     }
     if (threadIdx.x == 0) g.counter[b] = 0;
 }
@@ -1120,6 +1265,20 @@ static cudaStream_t capture_stream() {
     return s;
 }
 
+
+// The recycled-space kernels are instantiated for every k = 1..kMaxRecycle.
+template <typename S, int K> const void* recycle_kernel_k(bool combine) {
+    return combine ? (const void*)k_combine<S, K> : (const void*)k_bdots<S, K>;
+}
+template <typename S> const void* recycle_kernel(int k, bool combine) {
+    switch (k) {
+#define USV_K(K) case K: return recycle_kernel_k<S, K>(combine);
+        USV_K(1) USV_K(2) USV_K(3) USV_K(4) USV_K(5) USV_K(6) USV_K(7) USV_K(8)
+        USV_K(9) USV_K(10) USV_K(11) USV_K(12) USV_K(13) USV_K(14) USV_K(15) USV_K(16)
+#undef USV_K
+        default: return nullptr;
+    }
+}
 
 // Coefficients of the next recycled pair from one finished cycle's host-read
 // block: the harmonic Ritz update of GCRO-DR (Parks, de Sturler, Mackey,
@@ -1227,8 +1386,21 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     };
     dim3 grid_res, grid_dots, grid_orth, grid_upd, grid_gates;
     if (int e = grid_for((const void*)k_residual<ADJ, C2>, 256, 0, grid_res)) return e;
-    if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0, grid_dots))
+    if (kStreamDots) {
+        USV_CUDA_TRY(cudaFuncSetAttribute(k_dots_stream<R, S, ADJ>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(pipe_smem)));
+        if (int e = grid_for((const void*)k_dots_stream<R, S, ADJ>, kThreads, pipe_smem, grid_dots))
+            return e;
+    } else if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0,
+                                grid_dots)) {
         return e;
+    }
+    auto launch_dots = [&](cudaStream_t st, int j, int proj) {
+        if (kStreamDots)
+            k_dots_stream<R, S, ADJ><<<grid_dots, kThreads, pipe_smem, st>>>(opk, V, g, j, step, proj);
+        else
+            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
+    };
     if (int e = grid_for((const void*)k_orth<S>, kThreads, pipe_smem, grid_orth)) return e;
     if (int e = grid_for((const void*)k_update<S>, kThreads, pipe_smem, grid_upd)) return e;
     if (int e = grid_for((const void*)k_gates<ADJ>, 256, 0, grid_gates)) return e;
@@ -1238,16 +1410,21 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     const int kr = g.kr;
     dim3 grid_bd, grid_comb;
     size_t bd_smem = 0, comb_smem = 0;
+    const void* fn_bdots = nullptr;
+    const void* fn_comb = nullptr;
     if (kr > 0) {
         using T = typename Wide<S>::T;
         bd_smem = sizeof(T) * size_t(kr) * kBdTile + sizeof(double2) * size_t(g.m + 1) * kr;
         comb_smem = sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
-        USV_CUDA_TRY(cudaFuncSetAttribute(k_bdots<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        fn_bdots = recycle_kernel<S>(kr, false);
+        fn_comb = recycle_kernel<S>(kr, true);
+        if (!fn_bdots || !fn_comb) return USV_ERR_ARG;
+        USV_CUDA_TRY(cudaFuncSetAttribute(fn_bdots, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(bd_smem)));
-        USV_CUDA_TRY(cudaFuncSetAttribute(k_combine<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        USV_CUDA_TRY(cudaFuncSetAttribute(fn_comb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(comb_smem)));
-        if (int e = grid_for((const void*)k_bdots<S>, kThreads, bd_smem, grid_bd)) return e;
-        if (int e = grid_for((const void*)k_combine<S>, kThreads, comb_smem, grid_comb)) return e;
+        if (int e = grid_for(fn_bdots, kThreads, bd_smem, grid_bd)) return e;
+        if (int e = grid_for(fn_comb, kThreads, comb_smem, grid_comb)) return e;
     }
     // zero the state and the solution
     USV_CUDA_TRY(cudaMemsetAsync(ws + L.state_begin, 0, L.total - L.state_begin, strm));
@@ -1292,6 +1469,10 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     }
     const double vb = double(sizeof(C2)), nn = double(g.n);
     std::vector<double> fam_bytes;
+    // per measured interval: the Arnoldi step j (-1: none) and whether it
+    // only runs in recycled cycles (1) or with a new pair (2), so that the
+    // empty launches of a cycle count no bytes
+    std::vector<int> fam_step, fam_need;
     auto mark = [&](cudaStream_t st, int idx, bool capturing) {
         if (!prof) return cudaSuccess;
         return capturing ? cudaEventRecordWithFlags(ev[idx], st, cudaEventRecordExternal)
@@ -1301,60 +1482,93 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         int k = 0;
         fam.clear();
         fam_bytes.clear();
+        fam_step.clear();
+        fam_need.clear();
         USV_CUDA_TRY(mark(st, k++, capturing));
         if (kr > 0) {
             // new pair (when the host supplied coefficients), FP64 residual into
             // slot kc, projection of it on the recycled C
-            k_combine<S><<<grid_comb, kThreads, comb_smem, st>>>(V, g.n, g);
+            {
+                C2* vp = V;
+                GState gs = g;
+                long long nn_ = g.n;
+                void* args[] = {&vp, &nn_, &gs};
+                USV_CUDA_TRY(cudaLaunchKernel(fn_comb, grid_comb, dim3(kThreads), args, comb_smem, st));
+            }
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(6);
             fam_bytes.push_back(nn * vb * (2.0 * g.m + 2 * kr + 1));
+            fam_step.push_back(-1);
+            fam_need.push_back(2);
             k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
             fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
-            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, 0, step_d, 1);
+            fam_step.push_back(-1);
+            fam_need.push_back(0);
+            launch_dots(st, 0, 1);
             k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, 0, 1);
             USV_CUDA_TRY(mark(st, k++, capturing));
-            fam.push_back(6);
+            fam.push_back(7);
             fam_bytes.push_back(nn * vb * (2.0 * kr + 3));
+            fam_step.push_back(-1);
+            fam_need.push_back(1);
         }
         for (int j = 0; j < g.m; ++j) {
-            k_dots<R, S, ADJ, kDotsThreads>
-                <<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, 0);
+            launch_dots(st, j, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
             // read u_0..u_j (u_j also feeds the stencil) + node record, write w
             fam_bytes.push_back(nn * (vb * (j + 2) + 4.0 * sizeof(R)));
+            fam_step.push_back(j);
+            fam_need.push_back(0);
             k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(1);
             fam_bytes.push_back(nn * vb * (j + 3));
+            fam_step.push_back(j);
+            fam_need.push_back(0);
         }
         k_lsq<<<B, 128, lsq_smem, st>>>(g);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(2);
         fam_bytes.push_back(0.0);
+        fam_step.push_back(-1);
+        fam_need.push_back(0);
         k_update<S><<<grid_upd, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(3);
         fam_bytes.push_back(nn * (vb * g.m + 2 * sizeof(double2) + sizeof(double4)));
+        fam_step.push_back(-1);
+        fam_need.push_back(0);
         if (kr > 0) {
             // inner products for the harmonic Ritz step, then the host-read block
-            k_bdots<S><<<grid_bd, kThreads, bd_smem, st>>>(V, g.n, g);
+            {
+                C2* vp = V;
+                GState gs = g;
+                long long nn_ = g.n;
+                void* args[] = {&vp, &nn_, &gs};
+                USV_CUDA_TRY(cudaLaunchKernel(fn_bdots, grid_bd, dim3(kThreads), args, bd_smem, st));
+            }
             USV_CUDA_TRY(mark(st, k++, capturing));
-            fam.push_back(6);
+            fam.push_back(7);
             fam_bytes.push_back(nn * vb * (g.m + 1.0 + kr));
+            fam_step.push_back(-1);
+            fam_need.push_back(1);
             USV_CUDA_TRY(cudaMemcpyAsync(hb_pin.p, ws + L.hb, hb_bytes, cudaMemcpyDeviceToHost, st));
         } else {
             k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
             fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
+            fam_step.push_back(-1);
+            fam_need.push_back(0);
         }
         USV_CUDA_TRY(cudaGetLastError());
         return USV_OK;
     };
+    // measured cycle's recycled count and new-pair flag (first active RHS)
+    int meas_kc = 0, meas_combine = 0;
     auto accumulate = [&](std::vector<int>& active_counts) -> int {
         if (!prof) return USV_OK;
         for (size_t i = 0; i < fam.size(); ++i) {
@@ -1362,7 +1576,10 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             USV_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
             prof->milliseconds[fam[i]] += ms;
             prof->launches[fam[i]] += 1;
-            prof->bytes[fam[i]] += fam_bytes[i] * active_counts[0];
+            const bool idle = (fam_step[i] >= 0 && fam_step[i] < meas_kc) ||
+                              (fam_need[i] == 1 && meas_kc == 0) ||
+                              (fam_need[i] == 2 && !meas_combine);
+            if (!idle) prof->bytes[fam[i]] += fam_bytes[i] * active_counts[0];
         }
         return USV_OK;
     };
@@ -1452,6 +1669,12 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             if (e != cudaSuccess) { rc = set_last_cuda_error(e); break; }
             before = last;
             last = now;
+            for (int b = 0; b < B; ++b)
+                if (status[b] == ST_ACTIVE) {
+                    meas_kc = ctl[b * kCtl + CW_KC];
+                    meas_combine = ctl[b * kCtl + CW_COMBINE];
+                    break;
+                }
         }
         if (exec) {
             e = cudaGraphLaunch(exec, strm);
@@ -1563,6 +1786,27 @@ int usv_gmres_workspace_bytes(const usv_scene* scene, const usv_gmres_params* pa
     if (!bytes) return USV_ERR_ARG;
     const size_t vb = vector_bytes(params->precision);
     *bytes = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity, params->recycle).total;
+    return USV_OK;
+}
+
+int usv_harmonic_ritz(int m, int k, const double* G, const double* W, double* P, double* theta) {
+    if (m < 1 || k < 1 || k > m || !G || !W || !P || !theta) return USV_ERR_ARG;
+    using dense::cd;
+    const size_t n = size_t(m + 1) * m;
+    std::vector<cd> g(n), w(n), p, th;
+    for (size_t i = 0; i < n; ++i) {
+        g[i] = cd(G[2 * i], G[2 * i + 1]);
+        w[i] = cd(W[2 * i], W[2 * i + 1]);
+    }
+    if (!dense::harmonic_ritz(m, k, g, w, p, th)) return USV_ERR_NONFINITE;
+    for (size_t i = 0; i < size_t(m) * k; ++i) {
+        P[2 * i] = p[i].real();
+        P[2 * i + 1] = p[i].imag();
+    }
+    for (int i = 0; i < k; ++i) {
+        theta[2 * i] = th[i].real();
+        theta[2 * i + 1] = th[i].imag();
+    }
     return USV_OK;
 }
 
