@@ -23,6 +23,7 @@
 // Basis vectors are stored unnormalised with a scale sigma_t = 1/||u_t||.
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "dense.h"
@@ -45,6 +46,7 @@ enum {
     CW_SRC_VBUF,    // its Krylov buffer
     CW_SRC_KC,      // its recycled count
     CW_DST,         // pair buffer written by the combine
+    CW_HARVEST,     // 1: this cycle's data feeds a harmonic Ritz step
     kCtl
 };
 constexpr int kPairBufs = 3;   // pairs in use: this cycle's, the source cycle's, the new one
@@ -365,9 +367,27 @@ __device__ __forceinline__ void stage_vector(uint4* stg, const C2* base, int t, 
     cp_async_commit();
 }
 
-// Complex value c (0/1) of pair k of stage t % S, widened to double.
+// Arithmetic of the basis passes per storage type. bfloat16 values (8-bit
+// mantissa) are combined in fp32: their products, the orthogonalisation
+// update and per-lane partial sums of at most a few dozen terms are far more
+// precise than the stored values; every reduction across lanes, CTAs and
+// chunks stays FP64. complex64 and complex128 bases use FP64 throughout.
+// (Widening to FP64 costs conversion-unit throughput: with bfloat16 the FP64
+// dots saturated that unit in the Arnoldi kernel.)
+template <typename C2> struct MathT {
+    using T = double;
+    using T2 = double2;
+};
+template <> struct MathT<bf2> {
+    using T = float;
+    using T2 = float2;
+};
+__device__ __forceinline__ double2 to_d(double2 a);
+__device__ __forceinline__ float2 to_f(bf2 a) { return __bfloat1622float2(a); }
+
+// Complex value c (0/1) of pair k of stage t % S (in the pass arithmetic).
 template <typename C2>
-__device__ __forceinline__ double2 staged(const uint4* stg, int t, int k, int c);
+__device__ __forceinline__ typename MathT<C2>::T2 staged(const uint4* stg, int t, int k, int c);
 template <>
 __device__ __forceinline__ double2 staged<float2>(const uint4* stg, int t, int k, int c) {
     using P = Pipe<float2>;
@@ -376,13 +396,13 @@ __device__ __forceinline__ double2 staged<float2>(const uint4* stg, int t, int k
     return c ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
 }
 template <>
-__device__ __forceinline__ double2 staged<bf2>(const uint4* stg, int t, int k, int c) {
+__device__ __forceinline__ float2 staged<bf2>(const uint4* stg, int t, int k, int c) {
     using P = Pipe<bf2>;
     const int s = t % P::S;
     const unsigned* v = reinterpret_cast<const unsigned*>(
         &stg[(s * P::UNITS + (k >> 1)) * kThreads + threadIdx.x]);
     const unsigned raw = v[2 * (k & 1) + c];
-    return to_d(*reinterpret_cast<const bf2*>(&raw));
+    return to_f(*reinterpret_cast<const bf2*>(&raw));
 }
 
 __device__ __forceinline__ void st_pair(float2* p, double2 a, double2 b) {
@@ -411,6 +431,16 @@ __device__ __forceinline__ void ld_pair(const bf2* p, double2& a, double2& b) {
     b = to_d(*reinterpret_cast<const bf2*>(&raw.y));
 }
 __device__ __forceinline__ double2 rounded(const bf2*, double2 a) { return to_d(from_d<bf2>(a)); }
+__device__ __forceinline__ void st_pair(bf2* p, float2 a, float2 b) {
+    bf2 v[2] = {__float22bfloat162_rn(a), __float22bfloat162_rn(b)};
+    *reinterpret_cast<uint2*>(p) = *reinterpret_cast<const uint2*>(v);
+}
+__device__ __forceinline__ void ld_pair(const bf2* p, float2& a, float2& b) {
+    const uint2 raw = *reinterpret_cast<const uint2*>(p);
+    a = to_f(*reinterpret_cast<const bf2*>(&raw.x));
+    b = to_f(*reinterpret_cast<const bf2*>(&raw.y));
+}
+__device__ __forceinline__ float2 rounded(const bf2*, float2 a) { return to_f(__float22bfloat162_rn(a)); }
 // value actually stored (rounded to the vector precision)
 __device__ __forceinline__ double2 rounded(const float2*, double2 a) {
     return make_double2(double(float(a.x)), double(float(a.y)));
@@ -479,8 +509,11 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base0, const 
 // all warps work.
 constexpr int kDotUnroll = 8;
 constexpr int kDotsThreads = 512;
-// Dots phase form: warp tasks per vector (k_dots) or streamed per thread (k_dots_stream).
-constexpr bool kStreamDots = true;
+
+template <typename Y, typename C2> __device__ __forceinline__ Y as_ys(C2 v) { return v; }
+template <> __device__ __forceinline__ double2 as_ys<double2, float2>(float2 v) {
+    return make_double2(v.x, v.y);
+}
 
 template <typename C2> struct LaneLoad;
 template <> struct LaneLoad<bf2> {
@@ -488,9 +521,9 @@ template <> struct LaneLoad<bf2> {
     uint4 r;
     __device__ __forceinline__ void load(const bf2* p) { r = *reinterpret_cast<const uint4*>(p); }
     __device__ __forceinline__ void zero() { r = make_uint4(0u, 0u, 0u, 0u); }
-    __device__ __forceinline__ double2 get(int i) const {
+    __device__ __forceinline__ float2 get(int i) const {
         const unsigned v = i == 0 ? r.x : i == 1 ? r.y : i == 2 ? r.z : r.w;
-        return to_d(*reinterpret_cast<const bf2*>(&v));
+        return to_f(*reinterpret_cast<const bf2*>(&v));
     }
 };
 template <> struct LaneLoad<float2> {
@@ -514,7 +547,9 @@ template <> struct LaneLoad<double2> {
 // (stencil) into shared and global memory, then the dots <sigma_t u_t, w>,
 // t <= j, and ||w||^2. (A separate stencil kernel ahead of a streaming dots
 // kernel measured 9% slower per iteration at 128^3: the extra launch and the
-// re-read of w cost more than the overlap of the two phases gains.)
+// re-read of w cost more than the overlap of the two phases gains. Streaming
+// the dots per thread through the cp.async pipeline instead of warp tasks
+// measured the same for bfloat16 and 8% slower for complex64.)
 // proj = 1 (recycled cycles): no stencil; the dots alpha_t = <C_t, r> of the
 // cycle's first residual r (slot kc) with the recycled C_t, t < kc.
 template <typename R, typename S, bool ADJ, int NT>
@@ -530,7 +565,9 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     } else if (j < cb.kc) {
         return;
     }
-    __shared__ __align__(16) C2 ys[kChunk];
+    // w of the chunk in shared memory, widened once for complex64 (FP64 dots)
+    using YS = typename std::conditional<std::is_same<C2, float2>::value, double2, C2>::type;
+    __shared__ __align__(16) YS ys[kChunk];
     __shared__ double2 segsum[USV_MAX_RESTART + 2 > NT / 16 ? USV_MAX_RESTART + 2 : NT / 16];
     const long long N = op.n;
     const C2* uj = cb.V + (long long)j * g.nv;
@@ -560,12 +597,12 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
                     y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
                     w[n] = y;
                 }
-                ys[e] = y;
+                ys[e] = as_ys<YS>(y);
                 advance(p, step, op.nx, op.ny);
             }
         } else {
             for (int e = threadIdx.x; e < kChunk; e += NT)
-                ys[e] = e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0));
+                ys[e] = as_ys<YS>(e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0)));
         }
         __syncthreads();
         constexpr int NL = LaneLoad<C2>::NL;
@@ -574,7 +611,11 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         for (int task = warp; task < tasks_t * segs; task += nw) {
             const int t = task / segs, seg = task % segs;
             const int q0 = seg * per_seg, q1 = min(ngroups, q0 + per_seg);
-            double re = 0.0, im = 0.0;
+            // lane sums in the pass arithmetic (fp32 for bfloat16, <= 64 terms
+            // per lane and chunk), FP64 from the warp reduction on
+            using MT = typename MathT<C2>::T;
+            using M2 = typename MathT<C2>::T2;
+            MT lre = 0, lim = 0;
             if (t <= j) {
                 const C2* ut = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
                 for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
@@ -590,20 +631,20 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
                         const int q = min(qb + 32 * u, ngroups - 1);
 #pragma unroll
                         for (int c = 0; c < NL; ++c) {
-                            const double2 y = to_d(ys[NL * q + c]);
-                            const double2 av = a[u].get(c);
-                            re = fma(av.x, y.x, fma(av.y, y.y, re));
-                            im = fma(av.x, y.y, fma(-av.y, y.x, im));
+                            const M2 y = widen<M2>(ys[NL * q + c]);
+                            const M2 av = a[u].get(c);
+                            lre = fma(av.x, y.x, fma(av.y, y.y, lre));
+                            lim = fma(av.x, y.y, fma(-av.y, y.x, lim));
                         }
                     }
                 }
             } else {
                 for (int q = q0 + lane; q < q1; q += 32)
 #pragma unroll
-                    for (int c = 0; c < NL; ++c) re += cabs2(to_d(ys[NL * q + c]));
+                    for (int c = 0; c < NL; ++c) lre += cabs2(widen<M2>(ys[NL * q + c]));
             }
-            re = warp_sum(re);
-            im = warp_sum(im);
+            double re = warp_sum(double(lre));
+            double im = warp_sum(double(lim));
             if (lane == 0) segsum[task] = cadd(segsum[task], make_double2(re, im));
         }
     }
@@ -614,125 +655,6 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         for (int sg = 0; sg < segs; ++sg) {
             re += segsum[t * segs + sg].x;
             im += segsum[t * segs + sg].y;
-        }
-        if (t <= j) {
-            const double st = g.sigma[b * (g.m + 1) + t];
-            re *= st;
-            im *= st;
-        }
-        part[t] = make_double2(re, im);
-    }
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    const int nparts = int(gridDim.x);
-    for (int t = warp; t <= j + 1; t += nw) {
-        double re0 = 0.0, im0 = 0.0;
-        const double2* pt = g.partial + (long long)b * g.nblk * g.ps + t;
-        for (int q0 = 0; q0 < nparts; q0 += 32 * 4) {
-            double2 pv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int q = q0 + 32 * u + lane;
-                pv[u] = q < nparts ? ld_cg(pt + (long long)q * g.ps) : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                re0 += pv[u].x;
-                im0 += pv[u].y;
-            }
-        }
-        re0 = warp_sum(re0);
-        im0 = warp_sum(im0);
-        if (lane == 0) {
-            if (t > j) g.wnorm[b] = sqrt(re0);
-            else if (proj) g.alpha[(long long)b * g.kr + t] = make_double2(re0, im0);
-            else g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
-        }
-    }
-    if (threadIdx.x == 0) g.counter[b] = 0;
-}
-
-// Arnoldi step j, part 1, streaming form: the same stencil into shared and
-// global memory, then every thread takes the w values of its own node pairs
-// from shared memory and streams u_0..u_j through the cp.async pipeline (the
-// k_orth access pattern); the per-thread products of vector t are reduced
-// across the warp as soon as t is complete and added to a per-warp table in
-// chunk order (deterministic).
-template <typename R, typename S, bool ADJ>
-__global__ void __launch_bounds__(kThreads, 2) k_dots_stream(OpView<R> op, S* V, GState g, int j,
-                                                             Step step, int proj) {
-    using C2 = S;
-    const int b = blockIdx.y;
-    if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
-    const CycleBasis<C2> cb = cycle_basis(V, g, b);
-    if (proj) {
-        if (cb.kc == 0) return;
-        j = cb.kc - 1;
-    } else if (j < cb.kc) {
-        return;
-    }
-    extern __shared__ __align__(16) uint4 stg[];
-    __shared__ __align__(16) C2 ys[kChunk];
-    constexpr int nw = kThreads / 32;
-    __shared__ double2 tsum[nw][USV_MAX_RESTART + 2];
-    const long long N = op.n;
-    const C2* uj = cb.V + (long long)j * g.nv;
-    C2* w = cb.V + (long long)(j + 1) * g.nv;
-    const R sj = R(g.sigma[b * (g.m + 1) + j]);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int q = threadIdx.x; q < nw * (USV_MAX_RESTART + 2); q += kThreads)
-        (&tsum[0][0])[q] = make_double2(0.0, 0.0);
-    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
-        const long long n0 = (long long)ch * kChunk;
-        const int len = int(min((long long)kChunk, N - n0));
-        __syncthreads();  // the previous chunk is done with ys (and tsum is zeroed)
-        if (!proj) {
-            Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-#pragma unroll 4
-            for (int e = threadIdx.x; e < kChunk; e += kThreads) {
-                C2 y = from_d<C2>(make_double2(0.0, 0.0));
-                if (e < len) {
-                    const long long n = n0 + e;
-                    y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
-                    w[n] = y;
-                }
-                ys[e] = y;
-                advance(p, step, op.nx, op.ny);
-            }
-        } else {
-            for (int e = threadIdx.x; e < kChunk; e += kThreads)
-                ys[e] = e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0));
-        }
-        __syncthreads();
-        double2 y[kPairs][2];
-        double nrm = 0.0;
-#pragma unroll
-        for (int k = 0; k < kPairs; ++k)
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                y[k][c] = to_d(ys[pair_node<C2>(k) + c]);
-                nrm += cabs2(y[k][c]);
-            }
-        double pr = 0.0, pi = 0.0;
-        stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
-                         [&](int t, int k, int c, double2 v) {
-            pr = fma(v.x, y[k][c].x, fma(v.y, y[k][c].y, pr));
-            pi = fma(v.x, y[k][c].y, fma(-v.y, y[k][c].x, pi));
-            if (k == kPairs - 1 && c == 1) {  // vector t done for this thread
-                const double re = warp_sum(pr), im = warp_sum(pi);
-                if (lane == 0) tsum[warp][t] = cadd(tsum[warp][t], make_double2(re, im));
-                pr = pi = 0.0;
-            }
-        });
-        nrm = warp_sum(nrm);
-        if (lane == 0) tsum[warp][j + 1].x += nrm;
-    }
-    __syncthreads();
-    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
-    for (int t = threadIdx.x; t <= j + 1; t += kThreads) {
-        double re = 0.0, im = 0.0;
-        for (int q = 0; q < nw; ++q) {
-            re += tsum[q][t].x;
-            im += tsum[q][t].y;
         }
         if (t <= j) {
             const double st = g.sigma[b * (g.m + 1) + t];
@@ -790,26 +712,30 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     __shared__ double2 gsS[USV_MAX_RESTART + 1];
     __shared__ double gcS[USV_MAX_RESTART + 1];
     __shared__ double sh[32];
+    using M2 = typename MathT<C2>::T2;
+    __shared__ M2 hm[USV_MAX_RESTART + 2];
     const int m = g.m;
-    for (int t = threadIdx.x; t <= j; t += kThreads)
+    for (int t = threadIdx.x; t <= j; t += kThreads) {
         hs[t] = proj ? g.alpha[(long long)b * g.kr + t]
                      : cscale(g.H[((long long)b * m + j) * (m + 1) + t], g.sigma[b * (m + 1) + t]);
-    __syncthreads();  // hs visible
+        hm[t] = cmake<M2>(hs[t].x, hs[t].y);
+    }
+    __syncthreads();  // hs, hm visible
     double acc = 0.0;
     for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
         C2* w = cb.V + (long long)(j + 1) * g.nv + n0;
-        double2 u[kPairs][2];
+        M2 u[kPairs][2];
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
             const int e = pair_node<C2>(k);
             if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
-            else u[k][0] = u[k][1] = make_double2(0.0, 0.0);
+            else u[k][0] = u[k][1] = cmake<M2>(0.0, 0.0);
         }
         stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
-                         [&](int t, int k, int c, double2 vv) {
-            const double2 h = hs[t];
+                         [&](int t, int k, int c, M2 vv) {
+            const M2 h = hm[t];
             u[k][c].x -= h.x * vv.x - h.y * vv.y;
             u[k][c].y -= h.x * vv.y + h.y * vv.x;
         });
@@ -818,8 +744,8 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
             const int e = pair_node<C2>(k);
             if (e < len) {
                 st_pair(w + e, u[k][0], u[k][1]);
-                acc += cabs2(rounded(w, u[k][0]));
-                if (e + 1 < len) acc += cabs2(rounded(w, u[k][1]));
+                acc += double(cabs2(rounded(w, u[k][0])));
+                if (e + 1 < len) acc += double(cabs2(rounded(w, u[k][1])));
             }
         }
     }
@@ -986,8 +912,8 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) acc[k][0] = acc[k][1] = make_double2(0.0, 0.0);
         stream_basis<C2>(stg, cb.U + n0, cb.V + n0, cb.kc, g.nv, L - 1, len, false,
-                         [&](int t, int k, int c, double2 vv) {
-            acc[k][c] = cadd(acc[k][c], cmul(ys[t], vv));
+                         [&](int t, int k, int c, typename MathT<C2>::T2 vv) {
+            acc[k][c] = cadd(acc[k][c], cmul(ys[t], make_double2(vv.x, vv.y)));
         });
         double2* xb = x + b * ld + n0;
 #pragma unroll
@@ -1023,6 +949,7 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
     const CycleBasis<S> cb = cycle_basis(V, g, b);
     const int m = g.m;
     if (cb.kc != K) return;  // recycled cycles use all K vectors
+    if (!g.ctl[b * kCtl + CW_HARVEST]) return;
     constexpr int kc = K;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ut = reinterpret_cast<T*>(smem_raw);                                  // [kc][kBdTile]
@@ -1386,20 +1313,10 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     };
     dim3 grid_res, grid_dots, grid_orth, grid_upd, grid_gates;
     if (int e = grid_for((const void*)k_residual<ADJ, C2>, 256, 0, grid_res)) return e;
-    if (kStreamDots) {
-        USV_CUDA_TRY(cudaFuncSetAttribute(k_dots_stream<R, S, ADJ>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(pipe_smem)));
-        if (int e = grid_for((const void*)k_dots_stream<R, S, ADJ>, kThreads, pipe_smem, grid_dots))
-            return e;
-    } else if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0,
-                                grid_dots)) {
+    if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0, grid_dots))
         return e;
-    }
     auto launch_dots = [&](cudaStream_t st, int j, int proj) {
-        if (kStreamDots)
-            k_dots_stream<R, S, ADJ><<<grid_dots, kThreads, pipe_smem, st>>>(opk, V, g, j, step, proj);
-        else
-            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
+        k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
     };
     if (int e = grid_for((const void*)k_orth<S>, kThreads, pipe_smem, grid_orth)) return e;
     if (int e = grid_for((const void*)k_update<S>, kThreads, pipe_smem, grid_upd)) return e;
@@ -1554,7 +1471,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam.push_back(7);
             fam_bytes.push_back(nn * vb * (g.m + 1.0 + kr));
             fam_step.push_back(-1);
-            fam_need.push_back(1);
+            fam_need.push_back(3);
             USV_CUDA_TRY(cudaMemcpyAsync(hb_pin.p, ws + L.hb, hb_bytes, cudaMemcpyDeviceToHost, st));
         } else {
             k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
@@ -1568,7 +1485,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         return USV_OK;
     };
     // measured cycle's recycled count and new-pair flag (first active RHS)
-    int meas_kc = 0, meas_combine = 0;
+    int meas_kc = 0, meas_combine = 0, meas_harvest = 0;
     auto accumulate = [&](std::vector<int>& active_counts) -> int {
         if (!prof) return USV_OK;
         for (size_t i = 0; i < fam.size(); ++i) {
@@ -1578,7 +1495,8 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             prof->launches[fam[i]] += 1;
             const bool idle = (fam_step[i] >= 0 && fam_step[i] < meas_kc) ||
                               (fam_need[i] == 1 && meas_kc == 0) ||
-                              (fam_need[i] == 2 && !meas_combine);
+                              (fam_need[i] == 2 && !meas_combine) ||
+                              (fam_need[i] == 3 && (meas_kc == 0 || !meas_harvest));
             if (!idle) prof->bytes[fam[i]] += fam_bytes[i] * active_counts[0];
         }
         return USV_OK;
@@ -1659,6 +1577,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
                     u.kc = last[b].kc;
                 }
                 cw[CW_VBUF] = u.vbuf;
+                cw[CW_HARVEST] = cycle % every == 0;
                 pend[b].ready = false;
                 now[b] = u;
             }
@@ -1673,6 +1592,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
                 if (status[b] == ST_ACTIVE) {
                     meas_kc = ctl[b * kCtl + CW_KC];
                     meas_combine = ctl[b * kCtl + CW_COMBINE];
+                    meas_harvest = ctl[b * kCtl + CW_HARVEST];
                     break;
                 }
         }
