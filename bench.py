@@ -329,28 +329,39 @@ def run_ours(args):
                       "d2h_bytes_per_step": int(xh.nbytes), "steps": n_e2e,
                       "api": "HelmholtzB200Solver.solve_rhs(numpy)"}
 
-    # adjoint gradient: forward solve + A^H solve + phase VJP behind torch.autograd
+    # adjoint gradient: forward solve + A^H solve + phase VJP behind torch.autograd,
+    # in the mixed path and (unless --no-fp64) with the plain FP64 GMRES
     if not args.no_adjoint:
         from ultrasound_solver_b200.autograd import loss_of_field, phase_field
         from ultrasound_solver_b200.losses import ContrastRatioLoss
-        configure(args.precision)
         centre = (args.grid - 1) * solver.cfg.domain.dx / 2
         loss = ContrastRatioLoss(solver.cfg, (centre, centre, 0.080), 0.006, 0.010)
-        ph = torch.tensor(solver.transducers.phases, dtype=torch.float64, device="cuda",
-                          requires_grad=True)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        L = loss_of_field(phase_field(ph, solver), loss)
-        L.backward()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms_grad = max_over_ranks(e0.elapsed_time(e1), world)
+
+        def grad_once(precision):
+            configure(precision)
+            ph = torch.tensor(solver.transducers.phases, dtype=torch.float64, device="cuda",
+                              requires_grad=True)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            L = loss_of_field(phase_field(ph, solver), loss)
+            L.backward()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return max_over_ranks(e0.elapsed_time(e1), world), ph.grad.detach().clone()
+
+        ms_grad, grad = grad_once(args.precision)
         out["adjoint_grad"] = {"value": world * 1000.0 / ms_grad, "unit": "adjoint grads/s",
                                "ms_per_grad": ms_grad,
                                "loss": "-|u_t|^2 / mean_shell |u|^2 (target 80 mm above the array)",
-                               "grad_norm": float(torch.linalg.norm(ph.grad).item())}
+                               "grad_norm": float(torch.linalg.norm(grad).item())}
+        if not args.no_fp64:
+            ms64g, grad64 = grad_once("fp64")
+            out["adjoint_grad"]["fp64_grads_per_s"] = world * 1000.0 / ms64g
+            out["adjoint_grad"]["speedup_mixed_vs_fp64"] = ms64g / ms_grad
+            out["adjoint_grad"]["rel_err_vs_fp64"] = float(
+                (torch.linalg.norm(grad - grad64) / torch.linalg.norm(grad64)).item())
 
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_sample(args, cfg, fp64_iters)

@@ -39,6 +39,14 @@ template <> __host__ __device__ __forceinline__ double2 cmake<double2>(double re
     return make_double2(re, im);
 }
 
+template <typename C4> __host__ __device__ __forceinline__ C4 make_c4();
+template <> __host__ __device__ __forceinline__ float4 make_c4<float4>() {
+    return make_float4(0.f, 0.f, 0.f, 0.f);
+}
+template <> __host__ __device__ __forceinline__ double4 make_c4<double4>() {
+    return make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
 template <typename C, typename S> __host__ __device__ __forceinline__ C make_c2(S re, S im) {
     C r; r.x = re; r.y = im; return r;
 }
@@ -237,47 +245,170 @@ template <> __device__ __forceinline__ double harmonic2<double>(double a, double
 //   forward : y = u_n + R_n sum_j e_nj s_j u_j          (fixed row: y = u_n)
 //   adjoint : y = u_n + R'_n sum_{j not fixed} conj(e_nj) s'_j u_j
 // The unit diagonal follows from s = 1/(R A_ii) (iterative_solver.py:46-56).
+// The same row from the node's own record `me` and value `un` and a fetch
+// fetch(dir, r, u) of the neighbour record and value in direction
+// dir = 0..5 (x-, x+, y-, y+, z-, z+); directions outside the grid are never
+// fetched. Used with global-memory fetches (k_row) and with shared-memory /
+// register tiles (the z-marching stencil); the arithmetic is the same.
+template <typename R, bool ADJ, typename Fetch>
+__device__ __forceinline__ typename Tr<R>::c2 k_row_from(const OpView<R>& op, Node p,
+                                                        typename Tr<R>::c4 me,
+                                                        typename Tr<R>::c2 un, Fetch&& fetch) {
+    using C2 = typename Tr<R>::c2;
+    using C4 = typename Tr<R>::c4;
+    const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
+    if (!ADJ && fixed) return un;
+    const C2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
+    const C2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
+    C2 acc = cmake<C2>(0.0, 0.0);
+    auto edge = [&](int dir, C2 F, bool nb_fixed) {
+        if (ADJ && nb_fixed) return;
+        C4 r;
+        C2 uv;
+        fetch(dir, r, uv);
+        const R g = harmonic2<R>(me.x, r.x);
+        C2 e = cscale(F, g);
+        if (ADJ) e = cconj(e);
+        C2 sv = cmul(make_c2<C2>(r.z, r.w), uv);
+        acc = cadd(acc, cmul(e, sv));
+    };
+    if (p.i > 0)
+        edge(0, cmul(fyz, op.Q[0][p.i - 1]),
+             ADJ && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.i < op.nx - 1)
+        edge(1, cmul(fyz, op.Q[0][p.i]),
+             ADJ && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.j > 0)
+        edge(2, cmul(fxz, op.Q[1][p.j - 1]),
+             ADJ && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
+    if (p.j < op.ny - 1)
+        edge(3, cmul(fxz, op.Q[1][p.j]),
+             ADJ && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
+    if (p.k > 0)
+        edge(4, cmul(fxy, op.Q[2][p.k - 1]),
+             ADJ && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
+    if (p.k < op.nz - 1)
+        edge(5, cmul(fxy, op.Q[2][p.k]),
+             ADJ && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
+    return cadd(un, cscale(acc, me.y));
+}
+
 template <typename R, bool ADJ, typename S = typename Tr<R>::c2>
 __device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op, const S* __restrict__ u,
                                                     long long n, Node p) {
     using C2 = typename Tr<R>::c2;
     using C4 = typename Tr<R>::c4;
     const C2 un = widen<C2>(u[n]);
-    const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
-    if (!ADJ && fixed) return un;
-    const C4 me = op.rec[n];
-    const C2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
-    const C2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
-    C2 acc = cmake<C2>(0.0, 0.0);
-    auto edge = [&](long long m, C2 F, bool nb_fixed) {
-        if (ADJ && nb_fixed) return;
-        const C4 r = op.rec[m];
-        const R g = harmonic2<R>(me.x, r.x);
-        C2 e = cscale(F, g);
-        if (ADJ) e = cconj(e);
-        C2 sv = cmul(make_c2<C2>(r.z, r.w), widen<C2>(u[m]));
-        acc = cadd(acc, cmul(e, sv));
+    if (!ADJ && node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz)) return un;
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+    const long long off[6] = {-1, 1, -sy, sy, -sz, sz};
+    return k_row_from<R, ADJ>(op, p, op.rec[n], un, [&](int dir, C4& r, C2& uv) {
+        const long long m = n + off[dir];
+        r = op.rec[m];
+        uv = widen<C2>(u[m]);
+    });
+}
+
+// z-marching application of the K rows (2.5-D blocking): a CTA owns a
+// kZTX x kZTY tile of (i, j) columns and the planes [z0, z1). Each thread keeps
+// the record and value of its own column at z-1 .. z+2 in registers (two
+// planes of prefetch) and, on the tile edge, the halo node of the next plane;
+// the x/y neighbours of plane z come from a double-buffered shared-memory
+// tile with a one-node halo (one barrier per plane). Every node record and
+// value is read from HBM about once (plus the tile halo and the run ends) and
+// the neighbour accesses are register or shared-memory reads instead of
+// dependent global loads. out(n, value) receives the row of every grid node
+// of the tile column.
+constexpr int kZTX = 32, kZTY = 8;
+template <typename R> struct ZTile {
+    typename Tr<R>::c4 rec[2][kZTY + 2][kZTX + 2];
+    typename Tr<R>::c2 u[2][kZTY + 2][kZTX + 2];
+};
+template <typename R, bool ADJ, typename S, typename Out>
+__device__ __forceinline__ void zmarch_rows(const OpView<R>& op, const S* __restrict__ u, int tile,
+                                            int z0, int z1, ZTile<R>& sm, Out&& out) {
+    using C2 = typename Tr<R>::c2;
+    using C4 = typename Tr<R>::c4;
+    const int tiles_x = (op.nx + kZTX - 1) / kZTX;
+    const int bx = tile % tiles_x, by = tile / tiles_x;
+    const int tx = threadIdx.x % kZTX, ty = threadIdx.x / kZTX;
+    const int i = bx * kZTX + tx, j = by * kZTY + ty;
+    const bool in = i < op.nx && j < op.ny;
+    const long long sz = (long long)op.nx * op.ny;
+    auto load = [&](int ii, int jj, int z, C4& r, C2& v) {
+        if (ii >= 0 && ii < op.nx && jj >= 0 && jj < op.ny && z >= 0 && z < op.nz) {
+            const long long n = ii + (long long)op.nx * jj + sz * z;
+            r = op.rec[n];
+            v = widen<C2>(u[n]);
+        } else {
+            r = make_c4<C4>();
+            v = cmake<C2>(0.0, 0.0);
+        }
     };
-    const long long sx = 1, sy = op.nx, sz = (long long)op.nx * op.ny;
-    if (p.i > 0)
-        edge(n - sx, cmul(fyz, op.Q[0][p.i - 1]),
-             ADJ && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
-    if (p.i < op.nx - 1)
-        edge(n + sx, cmul(fyz, op.Q[0][p.i]),
-             ADJ && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
-    if (p.j > 0)
-        edge(n - sy, cmul(fxz, op.Q[1][p.j - 1]),
-             ADJ && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
-    if (p.j < op.ny - 1)
-        edge(n + sy, cmul(fxz, op.Q[1][p.j]),
-             ADJ && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
-    if (p.k > 0)
-        edge(n - sz, cmul(fxy, op.Q[2][p.k - 1]),
-             ADJ && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
-    if (p.k < op.nz - 1)
-        edge(n + sz, cmul(fxy, op.Q[2][p.k]),
-             ADJ && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
-    return cadd(un, cscale(acc, me.y));
+    // halo node of this thread (x edge, y edge), if any
+    const int hxi = tx == 0 ? i - 1 : (tx == kZTX - 1 ? i + 1 : -2);
+    const int hyj = ty == 0 ? j - 1 : (ty == kZTY - 1 ? j + 1 : -2);
+    const int hxs = tx == 0 ? 0 : kZTX + 1, hys = ty == 0 ? 0 : kZTY + 1;
+    C4 rp, rc, r1, r2, hxr, hyr, hxr1, hyr1;
+    C2 up, uc, u1, u2, hxu, hyu, hxu1, hyu1;
+    load(i, j, z0 - 1, rp, up);
+    load(i, j, z0, rc, uc);
+    load(i, j, z0 + 1, r1, u1);
+    if (hxi != -2) load(hxi, j, z0, hxr, hxu);
+    if (hyj != -2) load(i, hyj, z0, hyr, hyu);
+    for (int z = z0; z < z1; ++z) {
+        // prefetch: own column two planes ahead, halo one plane ahead
+        load(i, j, z + 2, r2, u2);
+        if (hxi != -2) load(hxi, j, z + 1, hxr1, hxu1);
+        if (hyj != -2) load(i, hyj, z + 1, hyr1, hyu1);
+        const int bf = (z - z0) & 1;
+        sm.rec[bf][ty + 1][tx + 1] = rc;
+        sm.u[bf][ty + 1][tx + 1] = uc;
+        if (hxi != -2) {
+            sm.rec[bf][ty + 1][hxs] = hxr;
+            sm.u[bf][ty + 1][hxs] = hxu;
+        }
+        if (hyj != -2) {
+            sm.rec[bf][hys][tx + 1] = hyr;
+            sm.u[bf][hys][tx + 1] = hyu;
+        }
+        __syncthreads();  // plane z visible; the other buffer was last read two planes ago
+        if (in) {
+            const Node p{i, j, z};
+            const C2 val = k_row_from<R, ADJ>(op, p, rc, uc, [&](int dir, C4& r, C2& v) {
+                switch (dir) {
+                    case 0: r = sm.rec[bf][ty + 1][tx]; v = sm.u[bf][ty + 1][tx]; break;
+                    case 1: r = sm.rec[bf][ty + 1][tx + 2]; v = sm.u[bf][ty + 1][tx + 2]; break;
+                    case 2: r = sm.rec[bf][ty][tx + 1]; v = sm.u[bf][ty][tx + 1]; break;
+                    case 3: r = sm.rec[bf][ty + 2][tx + 1]; v = sm.u[bf][ty + 2][tx + 1]; break;
+                    case 4: r = rp; v = up; break;
+                    default: r = r1; v = u1; break;
+                }
+            });
+            out(i + (long long)op.nx * j + sz * z, val);
+        }
+        rp = rc; up = uc;
+        rc = r1; uc = u1;
+        r1 = r2; u1 = u2;
+        hxr = hxr1; hxu = hxu1;
+        hyr = hyr1; hyu = hyu1;
+    }
+}
+
+// Grid of the z-marching kernels: tiles x runs of zseg planes, at most
+// `ctas` CTAs in total (one wave of resident CTAs).
+struct ZGrid {
+    int tiles, runs, zseg;
+};
+inline ZGrid zmarch_grid(int nx, int ny, int nz, int ctas) {
+    ZGrid z;
+    z.tiles = ((nx + kZTX - 1) / kZTX) * ((ny + kZTY - 1) / kZTY);
+    int runs = ctas / z.tiles;
+    runs = runs < 1 ? 1 : runs;
+    z.zseg = (nz + runs - 1) / runs;
+    z.zseg = z.zseg < 2 ? 2 : z.zseg;
+    z.runs = (nz + z.zseg - 1) / z.zseg;
+    return z;
 }
 
 // Row of the unscaled fp64 operator at node n applied to x (complex128).

@@ -77,6 +77,7 @@ class HelmholtzB200Solver:
             block_nodes=int(s.get("block_nodes", 0)),
             recycle=int(s.get("gmres_recycle", 0)),
             recycle_every=int(s.get("gmres_recycle_every", 1)),
+            batch_width=int(s.get("gmres_batch_width", 0)),
         )
 
     # ----------------------------------------------------------- scene

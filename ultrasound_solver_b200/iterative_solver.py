@@ -42,7 +42,7 @@ class B200IterativeSolver:
                  backward_error_tol: float = 1.0e-4, precision: str = "mixed",
                  full_cycles: bool = True, use_graph: bool = True, block_nodes: int = 0,
                  verbose: bool = False, profile: bool = False, recycle: int = 0,
-                 recycle_every: int = 1):
+                 recycle_every: int = 1, batch_width: int = 0):
         if str(precision).lower() not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         self.restart = int(restart)
@@ -55,6 +55,8 @@ class B200IterativeSolver:
         self.block_nodes = int(block_nodes)
         self.recycle = int(recycle)
         self.recycle_every = int(recycle_every)
+        # right-hand sides per launch (0: all of them); autotune.BatchTuner picks it
+        self.batch_width = int(batch_width)
         self.verbose = bool(verbose)
         self.profile = bool(profile)
         self.last_profile = None
@@ -93,12 +95,36 @@ class B200IterativeSolver:
         """Solve A x = rhs (or A^H x = rhs) on the device.
 
         rhs: complex128 device tensor of shape (N,) or (B, N) (row b is one
-        right-hand side). Returns x with the same shape.
+        right-hand side). Returns x with the same shape. With batch_width > 0
+        the right-hand sides go through the solver in launches of at most
+        batch_width (the stats then cover all of them).
         """
         squeeze = rhs.dim() == 1
         b = rhs.reshape(1, -1) if squeeze else rhs
         if b.shape[-1] != operator.n:
             raise ValueError("rhs length does not match the operator")
+        if 0 < self.batch_width < b.shape[0]:
+            parts, stats, hist, prof = [], [], [], None
+            for lo in range(0, b.shape[0], self.batch_width):
+                parts.append(self._solve_batch(operator, b[lo:lo + self.batch_width], adjoint,
+                                               raise_on_failure))
+                stats += self.last_stats
+                hist += self.last_history
+                if self.last_profile is not None:
+                    prof = prof or {k: dict(launches=0, ms=0.0, bytes=0.0) for k in self.last_profile}
+                    for k, v in self.last_profile.items():
+                        for f in v:
+                            prof[k][f] += v[f]
+            self.last_stats, self.last_history, self.last_profile = stats, hist, prof
+            self.last_iterations = max(s["iterations"] for s in stats)
+            self.last_scaled_residual = max(s["scaled_residual"] for s in stats)
+            self.last_backward_error = max(s["backward_error"] for s in stats)
+            return torch.cat(parts)
+        x = self._solve_batch(operator, b, adjoint, raise_on_failure)
+        return x[0] if squeeze else x
+
+    def _solve_batch(self, operator, b: torch.Tensor, adjoint: bool,
+                     raise_on_failure: bool) -> torch.Tensor:
         b = b.to(device=operator.device, dtype=torch.complex128).contiguous()
         nrhs = b.shape[0]
         x = torch.empty_like(b)
@@ -125,6 +151,7 @@ class B200IterativeSolver:
                                 initial_residual=s.initial_residual) for s in stats]
         self.last_history = [list(hist[k * hcap:k * hcap + min(s.cycles, hcap)])
                              for k, s in enumerate(stats)]
+        self.last_profile = None
         if prof is not None:
             self.last_profile = {name: dict(launches=prof.launches[i], ms=prof.milliseconds[i],
                                             bytes=prof.bytes[i])
@@ -143,4 +170,4 @@ class B200IterativeSolver:
             print(f"  --> GMRES iterations: {self.last_iterations} | scaled relative residual: "
                   f"{self.last_scaled_residual:.3e} | backward error: "
                   f"{self.last_backward_error:.3e}")
-        return x[0] if squeeze else x
+        return x

@@ -92,6 +92,38 @@ def config3(n=128, h=1e-3):
     return config1(n, h, array_n=16)
 
 
+def config2_basis_scene(n=96, h=1e-3):
+    """Config-2 basis scene: config-1 medium statistics, 16x16 array (10.5 mm pitch if it fits)."""
+    p, d = fit_array(16, n, h)
+    centre = (n - 1) * h / 2
+    sphere = {"type": "sphere", "center": [centre, centre, min(0.060, 0.6 * (n - 1) * h)],
+              "radius": min(0.015, 0.12 * (n - 1) * h), "smoothing_width_cells": 1.2,
+              "material": {"density": 1250.0, "sound_speed": 2200.0}}
+    return scene_dict(n, h, 16, p, d, boundaries={"+x": "reflecting"}, obstacle=sphere,
+                      solver={"gmres_restart": 20, "precision": "mixed"})
+
+
+def config2_scene_batch(count=32, seed=3, sizes=(48, 64, 80, 96, 112), h=1e-3):
+    """Config-2 uneven batch: grid edges drawn from `sizes`, a random sphere obstacle
+    (radius 8-20 mm, kept clear of the PML and the baffle) and an 8x8 array each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(sizes))
+        L = (n - 1) * h
+        p, d = fit_array(8, n, h)
+        inner = L - 2 * PML["cells"] * h
+        r = float(min(rng.uniform(0.008, 0.020), 0.2 * inner))
+        lo, hi = PML["cells"] * h + r + 2 * h, L - PML["cells"] * h - r - 2 * h
+        centre = [float(rng.uniform(lo, hi)), float(rng.uniform(lo, hi)),
+                  float(rng.uniform(max(lo, 0.4 * L), hi))]
+        sphere = {"type": "sphere", "center": centre, "radius": r, "smoothing_width_cells": 1.2,
+                  "material": {"density": 1250.0, "sound_speed": 2200.0}}
+        out.append(scene_dict(n, h, 8, p, d, boundaries={"+x": "reflecting"}, obstacle=sphere,
+                              solver={"gmres_restart": 20, "precision": "mixed"}))
+    return out
+
+
 def build_solver(cfg_dict, seed=0, device=None, random=True):
     """HelmholtzB200Solver for a scene dict; the obstacle is blended into the random medium."""
     import torch
