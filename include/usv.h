@@ -150,6 +150,14 @@ typedef struct usv_gmres_stats {
  * theta. USV_ERR_NONFINITE when the eigen-solve fails. */
 int usv_harmonic_ritz(int m, int k, const double* G, const double* W, double* P, double* theta);
 
+/* Homogeneous surface solver: for each of `modes` (x, y) modes the backward
+ * continued fraction of the z-axis operator (diag[nz], upper[nz-1],
+ * lower[nz-1]; upper[j] = Z[j, j+1], lower[j] = Z[j+1, j]) shifted by
+ * shift[mode]: history[j][mode] = u[j+1]/u[0], j < nz-1 (complex128 device
+ * arrays). Replaces _cuda_z_transfer (homogeneous_surface.py:41-85). */
+int usv_z_transfer(const void* shift, const void* diag, const void* upper, const void* lower,
+                   void* history, int modes, int nz, void* stream);
+
 /* library identity */
 int usv_abi_version(void);
 const char* usv_status_string(int status);

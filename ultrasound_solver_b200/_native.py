@@ -75,6 +75,7 @@ _SP = C.POINTER(Scene)
 _SIGNATURES = {
     "usv_abi_version": ([], _I),
     "usv_harmonic_ritz": ([_I, _I, _P, _P, _P, _P], _I),
+    "usv_z_transfer": ([_P, _P, _P, _P, _P, _I, _I, _P], _I),
     "usv_status_string": ([_I], C.c_char_p),
     "usv_device_info": ([C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)], _I),
     "usv_operator_bytes": ([_SP, C.POINTER(_SZ)], _I),

@@ -21,7 +21,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIBDIR = PKG / "_lib"
 LIBNAME = "libusv_b200.so"
-SOURCES = ("operator.cu", "gmres.cu", "scene.cu", "basis.cu", "losses.cu", "dense.cpp")
+SOURCES = ("operator.cu", "gmres.cu", "scene.cu", "basis.cu", "losses.cu", "surface.cu",
+           "dense.cpp")
 HEADERS = ("usv_internal.cuh", "dense.h")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

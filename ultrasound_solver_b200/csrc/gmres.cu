@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
     const double2* xb = x + b * ld;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     C2* v0 = cb.V + (long long)cb.kc * g.nv;
-    double acc = 0.0;
+    double acc = 0.0, acc_s = 0.0;
     for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * g.chunk;
         const long long n1 = min(n0 + g.chunk, op.n);
@@ -245,18 +245,28 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
             r = cscale(r, op.rec[n].y);
             const C2 rv = from_d<C2>(r);
             v0[n] = rv;
-            acc += cabs2(to_d(rv));
+            acc += cabs2(r);
+            acc_s += cabs2(to_d(rv));
         }
     }
     acc = block_sum(acc, sh);
+    acc_s = block_sum(acc_s, sh);
     if (threadIdx.x == 0)
-        g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
+        g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, acc_s);
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    // FP64 norm of the residual (the convergence test, like the final gate)
+    // and of its stored copy (the scale of the cycle's first basis vector)
     const double t = reduce_slot0(g, b, sh);
+    double ts = 0.0;
+    {
+        const double2* pp = g.partial + (long long)b * g.nblk * g.ps;
+        for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x) ts += ld_cg(pp + (long long)q * g.ps).y;
+        ts = block_sum(ts, sh);
+    }
     __shared__ int st_sh;
     const int m = g.m, kc = cb.kc;
     if (threadIdx.x == 0) {
-        const double beta = sqrt(t);
+        const double beta = sqrt(t), beta_s = sqrt(ts);
         if (first) {
             g.bnorm[b] = beta;
             g.atol[b] = g.rtol * beta;
@@ -271,13 +281,15 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
         }
         int st = ST_ACTIVE;
         if (!isfinite(beta)) st = ST_NONFINITE;
-        else if (beta <= g.atol[b]) st = ST_CONVERGED;
+        // (a hair inside atol: the final gate recomputes this norm with another
+        // summation order and must not miss rtol by a rounding)
+        else if (beta <= g.atol[b] * (1.0 - 1e-12)) st = ST_CONVERGED;
         else if (g.iters[b] >= g.maxiter) st = ST_MAXITER;
         g.status[b] = st;
         st_sh = st;
         if (st == ST_ACTIVE) {
-            g.sigma[b * (m + 1) + kc] = 1.0 / beta;
-            for (int i = 0; i <= m; ++i) g.g[b * (m + 1) + i] = make_double2(i == kc ? beta : 0.0, 0.0);
+            g.sigma[b * (m + 1) + kc] = 1.0 / beta_s;
+            for (int i = 0; i <= m; ++i) g.g[b * (m + 1) + i] = make_double2(i == kc ? beta_s : 0.0, 0.0);
             g.len[b] = m;
             g.ended[b] = 0;
         }
@@ -558,12 +570,12 @@ __global__ void __launch_bounds__(kZTX * kZTY) k_stencil25(OpView<R> op, S* V, G
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
     const CycleBasis<S> cb = cycle_basis(V, g, b);
     if (j < cb.kc) return;
-    __shared__ ZTile<R> sm;
+    __shared__ ZTile2<R> sm;
     const S* uj = cb.V + (long long)j * g.nv;
     S* w = cb.V + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
     const int z0 = blockIdx.y * zseg, z1 = min(op.nz, z0 + zseg);
-    zmarch_rows<R, ADJ>(op, uj, blockIdx.x, z0, z1, sm, [&](long long n, typename Tr<R>::c2 v) {
+    zmarch_rows2<R, ADJ>(op, uj, blockIdx.x, z0, z1, sm, [&](long long n, typename Tr<R>::c2 v) {
         w[n] = narrow<S>(cscale(v, sj));
     });
 }

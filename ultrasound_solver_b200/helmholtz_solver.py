@@ -4,7 +4,8 @@ Drop-in for the methods of src/algorithm/solvers/helmholtz_solver.py that the
 gpu_iterative backend serves (assemble_matrix, update_rhs, set_phases,
 set_material_fields, scene_fingerprint, solve, solve_rhs, solve_adjoint,
 material_vjp, build_phase_response_basis, invalidate_factorization,
-factorize, close), with the same argument shapes (Fortran voxel order),
+factorize, close, target_response, field_at, field_at_direct), with the same
+argument shapes (Fortran voxel order),
 return shapes, exceptions and stats. Differences, all deliberate:
 
 * the operator never exists as a CSR matrix: assembly is the per-node
@@ -65,6 +66,8 @@ class HelmholtzB200Solver:
         self._grid_definition = _as_dict(config.domain)
         self._source_definition = _as_dict(config.specs)
         self.condensed_solver = None
+        self._target_surface_solver = None
+        self._target_source_masses = None
         s = config.solver
         self.iterative_solver = B200IterativeSolver(
             restart=int(s.get("gmres_restart", 30)),
@@ -229,6 +232,8 @@ class HelmholtzB200Solver:
         self.assemble_matrix()
 
     def close(self):
+        self._target_surface_solver = None
+        self._target_source_masses = None
         self.invalidate_factorization()
 
     def _requested_backend(self) -> str:
@@ -237,6 +242,124 @@ class HelmholtzB200Solver:
             raise ValueError(f"solver.backend={backend!r} is not served by HelmholtzB200Solver; "
                              f"valid values are {list(VALID_BACKENDS)}")
         return backend
+
+    # ----------------------------------------------------------- homogeneous targets
+    # helmholtz_solver.py:79-226: exact target responses of homogeneous scenes
+    # through the surface Schur complement (homogeneous_surface.py).
+    def _ensure_target_surface_solver(self):
+        from .homogeneous_surface import HomogeneousSurfaceSolver
+        if self.cfg.obstacles or self.cfg.physics.material_field_file or self._material_fields is not None:
+            raise ValueError("Surface condensation requires a homogeneous medium")
+        if boundary_type(self.cfg.boundary_conditions.get("-z", "reflecting")) != "reflecting":
+            raise ValueError("Surface condensation requires a reflecting baffled -z face")
+        if self._target_surface_solver is not None:
+            return
+        self.assemble_matrix()
+        self._target_source_masses = self.sources.mass_matrix.T.cpu().numpy()
+        self._target_surface_solver = HomogeneousSurfaceSolver(
+            self.shape, self.cfg.domain.dx, self.cfg.frequency, self.cfg.physics.sound_speed,
+            self.cfg.physics.medium_density, self.cfg.boundary_conditions,
+            pml=self.cfg.solver.get("pml", {}), device=self.device)
+
+    def _local_target_points(self, points):
+        points = np.asarray(points, dtype=float)
+        local = points - self.origin
+        extent = np.asarray(self.cfg.domain.box_size, dtype=float)
+        if (points.ndim != 2 or points.shape[1] != 3 or not np.isfinite(points).all()
+                or np.any(local < -1e-12) or np.any(local > extent + 1e-12)):
+            raise ValueError("Targets must be finite physical coordinates inside the PDE domain")
+        pml = self.cfg.solver.get("pml", {}) or {}
+        cells = int(pml.get("cells", 0))
+        if cells:
+            faces = pml.get("faces", [f for f in FACES
+                                      if boundary_type(self.cfg.boundary_conditions[f]) == "open"])
+            thickness = cells * self.cfg.domain.dx
+            for face in faces:
+                axis = "xyz".index(face[1])
+                distance = local[:, axis] if face[0] == "-" else extent[axis] - local[:, axis]
+                if np.any(distance < thickness - 1e-12):
+                    raise ValueError("Target lies in PML; enlarge the physical interior")
+        return local
+
+    def _target_response_cache_fingerprint(self):
+        digest = hashlib.sha256()
+        here = Path(__file__)
+        for path in (here, here.with_name("homogeneous_surface.py"), here.with_name("scene.py")):
+            digest.update(path.read_bytes())
+        payload = {"model": self.MODEL_VERSION, "scene": self.scene_fingerprint(),
+                   "origin_m": self.origin.tolist(), "implementation_sha256": digest.hexdigest()}
+        return hashlib.sha256(json.dumps(payload, sort_keys=True,
+                                         separators=(",", ":")).encode()).hexdigest()
+
+    def _read_target_response_cache(self):
+        filename = str(self.cfg.solver.get("target_response_cache", "")).strip()
+        path = Path(filename) if filename else None
+        if path is None or not path.is_file():
+            return path, None
+        try:
+            with np.load(path, allow_pickle=False) as data:
+                if str(data["fingerprint"]) != self._target_response_cache_fingerprint():
+                    return path, None
+                points = np.asarray(data["points_m"], dtype=float)
+                response = np.asarray(data["response"], dtype=complex)
+        except (KeyError, OSError, ValueError):
+            return path, None
+        if (points.ndim != 2 or points.shape[1] != 3
+                or response.shape != (len(points), self.transducers.num_transducers)
+                or not np.isfinite(points).all() or not np.isfinite(response).all()):
+            return path, None
+        return path, (points, response)
+
+    def _write_target_response_cache(self, path, points, response):
+        if path is None:
+            return
+        path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = path.with_suffix(".tmp.npz")
+        np.savez_compressed(tmp, fingerprint=self._target_response_cache_fingerprint(),
+                            points_m=points, response=response)
+        tmp.replace(path)
+
+    def target_response(self, points):
+        """(P, M) target x channel responses of the discrete PDE (homogeneous scenes)."""
+        points = np.asarray(points, dtype=float)
+        local = self._local_target_points(points)
+        path, cached = self._read_target_response_cache()
+        channels = self.transducers.num_transducers
+        result = np.empty((len(points), channels), complex)
+        if cached is None:
+            cached_points = np.empty((0, 3), float)
+            cached_response = np.empty((0, channels), complex)
+        else:
+            cached_points, cached_response = cached
+        missing = []
+        for index, point in enumerate(points):
+            hit = np.flatnonzero(np.all(np.isclose(cached_points, point, rtol=0, atol=1e-12), axis=1))
+            if hit.size:
+                result[index] = cached_response[hit[0]]
+            else:
+                missing.append(index)
+        if missing:
+            self._ensure_target_surface_solver()
+            computed = self._target_surface_solver.flux_target_response(
+                self._target_source_masses, local[missing])
+            result[missing] = computed
+            self._write_target_response_cache(path, np.vstack((cached_points, points[missing])),
+                                              np.vstack((cached_response, computed)))
+        return result
+
+    def field_at(self, points, phases=None):
+        values = self.transducers.phases if phases is None else np.asarray(phases, dtype=float)
+        if values.shape != (self.transducers.num_transducers,) or not np.isfinite(values).all():
+            raise ValueError("phases must match the transducer array and be finite")
+        return self.target_response(points) @ np.exp(1j * values)
+
+    def field_at_direct(self, points, phases=None):
+        values = self.transducers.phases if phases is None else np.asarray(phases, dtype=float)
+        if values.shape != (self.transducers.num_transducers,) or not np.isfinite(values).all():
+            raise ValueError("phases must match the transducer array and be finite")
+        self._ensure_target_surface_solver()
+        self._target_surface_solver.solve_flux(self._target_source_masses, values)
+        return self._target_surface_solver.sample(self._local_target_points(points))
 
     # ----------------------------------------------------------- solves
     def solve(self) -> np.ndarray:

@@ -1,12 +1,18 @@
 """Small, self-terminating workloads for profiler captures.
 
     python -m ultrasound_solver_b200.profiling cycle --grid 128 --restart 112 --precision mixed
+    python -m ultrasound_solver_b200.profiling cycle --grid 128 --restart 40 --recycle 10 \
+        --cycles 4 --precision bf16
     python -m ultrasound_solver_b200.profiling stencil --grid 128
 
-`cycle` runs exactly one GMRES restart cycle (maxiter = restart, no CUDA
-graph, so every kernel is a separate launch) on the config-1 scene; skipping
-2*j launches of k_dots|k_orth lands on Arnoldi step j. `stencil` applies the
-K and A operators a few times. Both exit 0 without converging anything.
+`cycle` runs `--cycles` GMRES restart cycles (no CUDA graph, so every kernel
+is a separate launch) on the config-1 scene. Plain GMRES(m): skipping 2*j
+launches of k_dots|k_orth lands on Arnoldi step j of the first cycle. With
+--recycle k the first two cycles are plain and every later cycle launches
+k_dots|k_orth 2(m+1) times (the projection pair, then steps j = 0..m-1, the
+steps j < k returning at once): skipping 2(m+1)c + 2 + 2j lands on step j of
+cycle c >= 2. `stencil` applies the K and A operators a few times. Both exit
+0 without converging anything.
 """
 from __future__ import annotations
 
@@ -24,6 +30,9 @@ def main(argv=None):
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--restart", type=int, default=112)
     ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--recycle", type=int, default=0)
+    ap.add_argument("--recycle-every", type=int, default=1)
+    ap.add_argument("--cycles", type=int, default=1)
     args = ap.parse_args(argv)
     torch.cuda.set_device(0)
     solver = W.build_solver(W.config1(n=args.grid), seed=0)
@@ -31,7 +40,10 @@ def main(argv=None):
     rhs = solver.update_rhs_device()
     if args.what == "cycle":
         it = solver.iterative_solver
-        it.precision, it.restart, it.maxiter = args.precision, args.restart, args.restart
+        it.precision, it.restart = args.precision, args.restart
+        it.recycle, it.recycle_every = args.recycle, args.recycle_every
+        plain = min(args.cycles, 2) if args.recycle else args.cycles
+        it.maxiter = plain * args.restart + (args.cycles - plain) * (args.restart - args.recycle)
         it.rtol, it.use_graph = 1e-12, False
         it.solve(solver.operator, rhs, raise_on_failure=False)
         print("cycle", it.last_stats[0])
