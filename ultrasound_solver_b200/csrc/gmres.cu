@@ -570,12 +570,12 @@ __global__ void __launch_bounds__(kZTX * kZTY) k_stencil25(OpView<R> op, S* V, G
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
     const CycleBasis<S> cb = cycle_basis(V, g, b);
     if (j < cb.kc) return;
-    __shared__ ZTile2<R> sm;
+    __shared__ ZTile<R> sm;
     const S* uj = cb.V + (long long)j * g.nv;
     S* w = cb.V + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
     const int z0 = blockIdx.y * zseg, z1 = min(op.nz, z0 + zseg);
-    zmarch_rows2<R, ADJ>(op, uj, blockIdx.x, z0, z1, sm, [&](long long n, typename Tr<R>::c2 v) {
+    zmarch_rows<R, ADJ>(op, uj, blockIdx.x, z0, z1, sm, [&](long long n, typename Tr<R>::c2 v) {
         w[n] = narrow<S>(cscale(v, sj));
     });
 }

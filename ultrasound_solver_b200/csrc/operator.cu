@@ -225,16 +225,16 @@ __global__ void __launch_bounds__(256) k_apply_k(OpView<R> op, const typename Tr
 // y = K x through the z-marching tile kernel (usv_internal.cuh: zmarch_rows).
 // usv_operator_apply K / K^H: z-marching kernel for complex128 (74 vs 97 us at
 // 128^3), the direct kernel for complex64 (35 vs 40 us).
-constexpr bool kZMarch64 = true, kZMarch32 = true;
+constexpr bool kZMarch64 = true, kZMarch32 = false;
 template <typename R, bool ADJ>
 __global__ void __launch_bounds__(kZTX * kZTY) k_apply_k25(OpView<R> op, const typename Tr<R>::c2* x,
                                                            typename Tr<R>::c2* y, long long ld,
                                                            int zseg) {
-    __shared__ ZTile2<R> sm;
+    __shared__ ZTile<R> sm;
     const int b = blockIdx.z;
     auto* yb = y + b * ld;
     const int z0 = blockIdx.y * zseg, z1 = min(op.nz, z0 + zseg);
-    zmarch_rows2<R, ADJ>(op, x + b * ld, blockIdx.x, z0, z1, sm,
+    zmarch_rows<R, ADJ>(op, x + b * ld, blockIdx.x, z0, z1, sm,
                         [&](long long n, typename Tr<R>::c2 v) { yb[n] = v; });
 }
 

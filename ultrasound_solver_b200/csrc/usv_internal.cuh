@@ -395,136 +395,6 @@ __device__ __forceinline__ void zmarch_rows(const OpView<R>& op, const S* __rest
     }
 }
 
-// Faster z-marching form. Each node's scaled value s_n u_n (the Jacobi
-// column scale times the vector) is formed once, when its plane is loaded,
-// instead of once per neighbour; the tile then holds (rho, s u) per node. The
-// edge factors of a column are split into a per-column part (T and Q of the
-// x and y axes) and a per-plane part (T_z, Q_z, uniform across the CTA), and
-// where all of them are real (outside every PML layer) the edge weights are
-// real. Same operator as k_row, different rounding order.
-template <typename R> struct ZTile2 {
-    typename Tr<R>::c2 su[2][kZTY + 2][kZTX + 2];
-    R rho[2][kZTY + 2][kZTX + 2];
-};
-template <typename R> struct ZPoint {
-    R rho, rs;                    // density, row scale
-    typename Tr<R>::c2 su, uv;    // s u, u
-};
-template <typename R, bool ADJ, typename S, typename Out>
-__device__ __forceinline__ void zmarch_rows2(const OpView<R>& op, const S* __restrict__ u, int tile,
-                                             int z0, int z1, ZTile2<R>& sm, Out&& out) {
-    using C2 = typename Tr<R>::c2;
-    using C4 = typename Tr<R>::c4;
-    using P = ZPoint<R>;
-    const int tiles_x = (op.nx + kZTX - 1) / kZTX;
-    const int bx = tile % tiles_x, by = tile / tiles_x;
-    const int tx = threadIdx.x % kZTX, ty = threadIdx.x / kZTX;
-    const int i = bx * kZTX + tx, j = by * kZTY + ty;
-    const bool in = i < op.nx && j < op.ny;
-    const long long sz = (long long)op.nx * op.ny;
-    const C2 zero = cmake<C2>(0.0, 0.0);
-    auto load = [&](int ii, int jj, int z) {
-        P p;
-        if (ii >= 0 && ii < op.nx && jj >= 0 && jj < op.ny && z >= 0 && z < op.nz) {
-            const long long n = ii + (long long)op.nx * jj + sz * z;
-            const C4 r = op.rec[n];
-            const C2 v = widen<C2>(u[n]);
-            p.rho = r.x;
-            p.rs = r.y;
-            p.su = cmul(make_c2<C2>(r.z, r.w), v);
-            p.uv = v;
-        } else {
-            p.rho = R(1);
-            p.rs = R(0);
-            p.su = p.uv = zero;
-        }
-        return p;
-    };
-    // per-column edge factors (x, y edges without T_z; z edges without Q_z)
-    const int ic = i < op.nx ? i : op.nx - 1, jc = j < op.ny ? j : op.ny - 1;
-    const bool hxm = ic > 0, hxp = ic < op.nx - 1, hym = jc > 0, hyp = jc < op.ny - 1;
-    const C2 Tx = op.T[0][ic], Ty = op.T[1][jc];
-    const C2 axm = hxm ? cmul(Ty, op.Q[0][ic - 1]) : zero, axp = hxp ? cmul(Ty, op.Q[0][ic]) : zero;
-    const C2 aym = hym ? cmul(Tx, op.Q[1][jc - 1]) : zero, ayp = hyp ? cmul(Tx, op.Q[1][jc]) : zero;
-    const C2 fxy = cmul(Tx, Ty);
-    const bool col_real = axm.y == 0 && axp.y == 0 && aym.y == 0 && ayp.y == 0 && fxy.y == 0;
-    const bool soft = op.soft != 0;
-    const int hxi = tx == 0 ? i - 1 : (tx == kZTX - 1 ? i + 1 : -2);
-    const int hyj = ty == 0 ? j - 1 : (ty == kZTY - 1 ? j + 1 : -2);
-    const int hxs = tx == 0 ? 0 : kZTX + 1, hys = ty == 0 ? 0 : kZTY + 1;
-    P pp = load(i, j, z0 - 1), pc = load(i, j, z0), p1 = load(i, j, z0 + 1), p2;
-    P hx, hy, hx1, hy1;
-    if (hxi != -2) hx = load(hxi, j, z0);
-    if (hyj != -2) hy = load(i, hyj, z0);
-    for (int z = z0; z < z1; ++z) {
-        p2 = load(i, j, z + 2);
-        if (hxi != -2) hx1 = load(hxi, j, z + 1);
-        if (hyj != -2) hy1 = load(i, hyj, z + 1);
-        const int bf = (z - z0) & 1;
-        sm.su[bf][ty + 1][tx + 1] = pc.su;
-        sm.rho[bf][ty + 1][tx + 1] = pc.rho;
-        if (hxi != -2) {
-            sm.su[bf][ty + 1][hxs] = hx.su;
-            sm.rho[bf][ty + 1][hxs] = hx.rho;
-        }
-        if (hyj != -2) {
-            sm.su[bf][hys][tx + 1] = hy.su;
-            sm.rho[bf][hys][tx + 1] = hy.rho;
-        }
-        __syncthreads();  // plane z visible; the other buffer was last read two planes ago
-        if (in) {
-            const long long n = i + (long long)op.nx * j + sz * z;
-            const bool fixed = soft && node_fixed(op.soft, i, j, z, op.nx, op.ny, op.nz);
-            if (!ADJ && fixed) {
-                out(n, pc.uv);
-            } else {
-                const bool hzm = z > 0, hzp = z < op.nz - 1;
-                const C2 Tz = op.T[2][z];
-                const C2 Qzm = hzm ? op.Q[2][z - 1] : zero, Qzp = hzp ? op.Q[2][z] : zero;
-                auto nbf = [&](int ii, int jj, int kk) {
-                    return ADJ && soft && node_fixed(op.soft, ii, jj, kk, op.nx, op.ny, op.nz);
-                };
-                const bool fm[6] = {hxm && nbf(i - 1, j, z), hxp && nbf(i + 1, j, z),
-                                    hym && nbf(i, j - 1, z), hyp && nbf(i, j + 1, z),
-                                    hzm && nbf(i, j, z - 1), hzp && nbf(i, j, z + 1)};
-                const bool has[6] = {hxm, hxp, hym, hyp, hzm, hzp};
-                const R rn[6] = {sm.rho[bf][ty + 1][tx], sm.rho[bf][ty + 1][tx + 2],
-                                 sm.rho[bf][ty][tx + 1], sm.rho[bf][ty + 2][tx + 1], pp.rho, p1.rho};
-                const C2 sn[6] = {sm.su[bf][ty + 1][tx], sm.su[bf][ty + 1][tx + 2],
-                                  sm.su[bf][ty][tx + 1], sm.su[bf][ty + 2][tx + 1], pp.su, p1.su};
-                C2 acc = zero;
-                if (col_real && Tz.y == 0 && Qzm.y == 0 && Qzp.y == 0) {
-                    const R F[6] = {axm.x * Tz.x, axp.x * Tz.x, aym.x * Tz.x, ayp.x * Tz.x,
-                                    fxy.x * Qzm.x, fxy.x * Qzp.x};
-#pragma unroll
-                    for (int d = 0; d < 6; ++d)
-                        if (has[d] && !fm[d]) {
-                            const R e = F[d] * harmonic2<R>(pc.rho, rn[d]);
-                            acc.x += e * sn[d].x;
-                            acc.y += e * sn[d].y;
-                        }
-                } else {
-                    const C2 F[6] = {cmul(axm, Tz), cmul(axp, Tz), cmul(aym, Tz), cmul(ayp, Tz),
-                                     cmul(fxy, Qzm), cmul(fxy, Qzp)};
-#pragma unroll
-                    for (int d = 0; d < 6; ++d)
-                        if (has[d] && !fm[d]) {
-                            C2 e = cscale(F[d], harmonic2<R>(pc.rho, rn[d]));
-                            if (ADJ) e = cconj(e);
-                            acc = cadd(acc, cmul(e, sn[d]));
-                        }
-                }
-                out(n, cadd(pc.uv, cscale(acc, pc.rs)));
-            }
-        }
-        pp = pc;
-        pc = p1;
-        p1 = p2;
-        hx = hx1;
-        hy = hy1;
-    }
-}
-
 // Grid of the z-marching kernels: tiles x runs of zseg planes, at most
 // `ctas` CTAs in total (one wave of resident CTAs).
 struct ZGrid {
