@@ -12,7 +12,7 @@ phase vector per right-hand side). Inputs are synthetic.
 Our arm: mixed-precision batched solves on the matrix-free sm_100a stencil:
 bfloat16 Krylov vectors (fp32 stencil, FP64 dots, Hessenberg/Givens, FP64
 true residual and solution update at every restart) with deflated restarting
-(GCRO-DR(40, 10): 10 harmonic Ritz vectors recycled across restarts). The
+(GCRO-DR(36, 8): 8 harmonic Ritz vectors recycled across restarts). The
 plain FP64 GMRES(30) of the same stencil (the reference's algorithm in FP64)
 is timed once beside it on the first right-hand side, and the relative L2
 difference between the two solutions is reported. `--impl reference` times
@@ -61,8 +61,8 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--grid", type=int, default=128)
-    ap.add_argument("--restart", type=int, default=40)
-    ap.add_argument("--recycle", type=int, default=10,
+    ap.add_argument("--restart", type=int, default=36)
+    ap.add_argument("--recycle", type=int, default=8,
                     help="harmonic Ritz vectors recycled across restarts (0: plain GMRES)")
     ap.add_argument("--recycle-every", type=int, default=2)
     ap.add_argument("--precision", default="bf16", choices=("bf16", "mixed"))
