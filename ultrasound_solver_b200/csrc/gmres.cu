@@ -655,7 +655,42 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
             using MT = typename MathT<C2>::T;
             using M2 = typename MathT<C2>::T2;
             MT lre = 0, lim = 0;
-            if (t <= j) {
+            if constexpr (std::is_same<C2, bf2>::value) {
+                // bfloat16 x bfloat16 products straight from the packed words
+                // (exact in fp32), four fp32 lane sums: Re = rr + ii, Im = ri - ir
+                float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
+                const uint4* yw = reinterpret_cast<const uint4*>(ys);
+                if (t <= j) {
+                    const uint4* ut = reinterpret_cast<const uint4*>(
+                        (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0);
+                    for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
+                        uint4 a[kDotUnroll];
+#pragma unroll
+                        for (int u = 0; u < kDotUnroll; ++u) {
+                            const int q = qb + 32 * u;
+                            a[u] = q < q1 ? ut[q] : make_uint4(0u, 0u, 0u, 0u);
+                        }
+#pragma unroll
+                        for (int u = 0; u < kDotUnroll; ++u) {
+                            const uint4 y = yw[min(qb + 32 * u, ngroups - 1)];
+                            bf_mac(rr, ii, ri, ir, a[u].x, y.x);
+                            bf_mac(rr, ii, ri, ir, a[u].y, y.y);
+                            bf_mac(rr, ii, ri, ir, a[u].z, y.z);
+                            bf_mac(rr, ii, ri, ir, a[u].w, y.w);
+                        }
+                    }
+                } else {
+                    for (int q = q0 + lane; q < q1; q += 32) {
+                        const uint4 y = yw[q];
+                        bf_sq(rr, ii, y.x);
+                        bf_sq(rr, ii, y.y);
+                        bf_sq(rr, ii, y.z);
+                        bf_sq(rr, ii, y.w);
+                    }
+                }
+                lre = rr + ii;
+                lim = ri - ir;
+            } else if (t <= j) {
                 const C2* ut = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
                 for (int qb = q0 + lane; qb < q1; qb += 32 * kDotUnroll) {
                     LaneLoad<C2> a[kDotUnroll];
@@ -1485,8 +1520,9 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             launch_dots(st, j, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
-            // read u_0..u_j (u_j also feeds the stencil) + node record, write w
-            fam_bytes.push_back(nn * (vb * (j + 2) + 4.0 * sizeof(R)));
+            // read u_0..u_j (u_j also feeds the stencil) + the row coefficients
+            // (complex64: 48 B) or node record (complex128: 32 B), write w
+            fam_bytes.push_back(nn * (vb * (j + 2) + (sizeof(R) == 4 ? 48.0 : 32.0)));
             fam_step.push_back(j);
             fam_need.push_back(0);
             k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j, 0);

@@ -186,6 +186,34 @@ __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
     }
 }
 
+// Complex64 row coefficients c_nd = R_n e_nd s_d (conj(e_nd) and the adjoint
+// scalings for K'), evaluated in FP64 by the same row code as the FP64
+// operator with a unit value in direction d only, then rounded once to fp32.
+// The complex64 rows (usv_internal.cuh: k_row_cf) then cost six complex
+// multiply-adds per node.
+template <bool ADJ>
+__global__ void __launch_bounds__(256) k_coef(OpView<double> op, float4* cf) {
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
+         n += (long long)gridDim.x * blockDim.x) {
+        const Node p = decode(n, op.nx, op.ny);
+        const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+        const long long off[6] = {-1, 1, -sy, sy, -sz, sz};
+        const double4 me = op.rec[n];
+        float2 c[6];
+        for (int d = 0; d < 6; ++d) {
+            const double2 v = k_row_from<double, ADJ>(
+                op, p, me, make_double2(0.0, 0.0), [&](int dir, double4& r, double2& uv) {
+                    r = op.rec[n + off[dir]];
+                    uv = make_double2(dir == d ? 1.0 : 0.0, 0.0);
+                });
+            c[d] = make_float2(float(v.x), float(v.y));
+        }
+        cf[3 * n] = make_float4(c[0].x, c[0].y, c[1].x, c[1].y);
+        cf[3 * n + 1] = make_float4(c[2].x, c[2].y, c[3].x, c[3].y);
+        cf[3 * n + 2] = make_float4(c[4].x, c[4].y, c[5].x, c[5].y);
+    }
+}
+
 static unsigned grid_for(long long n, int threads = 256) {
     long long b = (n + threads - 1) / threads;
     if (b > 148LL * 32) b = 148LL * 32;
@@ -342,6 +370,11 @@ int usv_operator_build(const usv_scene* scene, const double* rho, const double* 
     a.rec32a = reinterpret_cast<float4*>(buf + L.rec32a);
     a.flag = reinterpret_cast<int*>(buf + L.flag);
     k_build<<<grid_for(a.op.n), 256, 0, strm>>>(a);
+    USV_CUDA_TRY(cudaGetLastError());
+    k_coef<false><<<grid_for(a.op.n), 256, 0, strm>>>(
+        make_view<double>(s, op_buf, false), reinterpret_cast<float4*>(buf + L.cf32f));
+    k_coef<true><<<grid_for(a.op.n), 256, 0, strm>>>(
+        make_view<double>(s, op_buf, true), reinterpret_cast<float4*>(buf + L.cf32a));
     USV_CUDA_TRY(cudaGetLastError());
     int flag = 0;
     USV_CUDA_TRY(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, strm));

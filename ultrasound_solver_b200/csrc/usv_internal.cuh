@@ -111,12 +111,38 @@ template <> __device__ __forceinline__ float2 narrow<float2>(float2 a) { return 
 template <> __device__ __forceinline__ double2 narrow<double2>(double2 a) { return a; }
 template <> __device__ __forceinline__ bf2 narrow<bf2>(float2 a) { return __float22bfloat162_rn(a); }
 
+// Mixed-precision multiply-adds on packed bfloat16 complex words {re, im}
+// (PTX fma.rn.f32.bf16, sm_100: bf16 x bf16 products, exact in fp32, added to
+// an fp32 sum with one rounding). bf_mac accumulates the four real products of
+// conj(v) y: Re = rr + ii, Im = ri - ir.
+__device__ __forceinline__ void bf_mac(float& rr, float& ii, float& ri, float& ir, unsigned v,
+                                       unsigned y) {
+    asm("{\n\t.reg .b16 vl, vh, yl, yh;\n\t"
+        "mov.b32 {vl, vh}, %4;\n\t"
+        "mov.b32 {yl, yh}, %5;\n\t"
+        "fma.rn.f32.bf16 %0, vl, yl, %0;\n\t"
+        "fma.rn.f32.bf16 %1, vh, yh, %1;\n\t"
+        "fma.rn.f32.bf16 %2, vl, yh, %2;\n\t"
+        "fma.rn.f32.bf16 %3, vh, yl, %3;\n\t}"
+        : "+f"(rr), "+f"(ii), "+f"(ri), "+f"(ir)
+        : "r"(v), "r"(y));
+}
+// |y|^2 of a packed word: rr += re^2, ii += im^2
+__device__ __forceinline__ void bf_sq(float& rr, float& ii, unsigned y) {
+    asm("{\n\t.reg .b16 yl, yh;\n\t"
+        "mov.b32 {yl, yh}, %2;\n\t"
+        "fma.rn.f32.bf16 %0, yl, yl, %0;\n\t"
+        "fma.rn.f32.bf16 %1, yh, yh, %1;\n\t}"
+        : "+f"(rr), "+f"(ii)
+        : "r"(y));
+}
+
 // ---------------------------------------------------------------- layout
 // Byte offsets of the operator buffer. Everything is derived from the scene,
 // so host and device agree without storing the layout itself.
 struct Layout {
     size_t tab64[3], q64[3], tab32[3], q32[3];
-    size_t rec64f, rec64a, d64, rec32f, rec32a, flag;
+    size_t rec64f, rec64a, d64, rec32f, rec32a, cf32f, cf32a, flag;
     size_t total;
 };
 
@@ -138,6 +164,10 @@ inline Layout make_layout(const usv_scene& s) {
     L.d64 = off;    off = align_up(off + sizeof(double2) * n);
     L.rec32f = off; off = align_up(off + sizeof(float4) * n);
     L.rec32a = off; off = align_up(off + sizeof(float4) * n);
+    // complex64 row coefficients c_nd = R_n e_nd s_d of the six neighbour
+    // directions, three float4 per node (forward, adjoint)
+    L.cf32f = off;  off = align_up(off + 3 * sizeof(float4) * n);
+    L.cf32a = off;  off = align_up(off + 3 * sizeof(float4) * n);
     L.flag = off;   off = align_up(off + 64);
     L.total = off;
     return L;
@@ -155,6 +185,7 @@ template <typename R> struct OpView {
     const C2* Q[3];         // Q_a[i] = 1 / (0.5 (s_a[i] + s_a[i+1]) dx^2)
     const C4* rec;          // {rho, R, s.re, s.im} (forward or adjoint)
     const double2* d;       // diagonal A_ii (fp64 path only)
+    const float4* cf;       // complex64 path: row coefficients, 3 float4 per node
 };
 
 inline unsigned soft_mask(const usv_scene& s) {
@@ -180,6 +211,7 @@ inline OpView<R> make_view(const usv_scene& s, const void* buf, bool adjoint) {
     size_t rec = dbl ? (adjoint ? L.rec64a : L.rec64f) : (adjoint ? L.rec32a : L.rec32f);
     v.rec = reinterpret_cast<const typename OpView<R>::C4*>(b + rec);
     v.d = reinterpret_cast<const double2*>(b + L.d64);
+    v.cf = dbl ? nullptr : reinterpret_cast<const float4*>(b + (adjoint ? L.cf32a : L.cf32f));
     return v;
 }
 
@@ -293,20 +325,54 @@ __device__ __forceinline__ typename Tr<R>::c2 k_row_from(const OpView<R>& op, No
     return cadd(un, cscale(acc, me.y));
 }
 
+// Complex64 row from the precomputed coefficients (operator.cu: k_coef):
+// y = u_n + sum_d c_nd u_d over the six neighbour directions. A missing
+// neighbour (grid edge) and every edge of a fixed forward row carry a zero
+// coefficient, so their loads are redirected to u_n, which exists and is finite.
+template <typename S>
+__device__ __forceinline__ float2 k_row_cf(const OpView<float>& op, const S* __restrict__ u,
+                                           long long n, Node p) {
+    const float4* c = op.cf + 3 * n;
+    const float4 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2);
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+    const float2 u0 = widen<float2>(u[p.i > 0 ? n - 1 : n]);
+    const float2 u1 = widen<float2>(u[p.i < op.nx - 1 ? n + 1 : n]);
+    const float2 u2 = widen<float2>(u[p.j > 0 ? n - sy : n]);
+    const float2 u3 = widen<float2>(u[p.j < op.ny - 1 ? n + sy : n]);
+    const float2 u4 = widen<float2>(u[p.k > 0 ? n - sz : n]);
+    const float2 u5 = widen<float2>(u[p.k < op.nz - 1 ? n + sz : n]);
+    float2 y = widen<float2>(u[n]);
+    auto mac = [&](float cr, float ci, float2 v) {
+        y.x = fmaf(cr, v.x, fmaf(-ci, v.y, y.x));
+        y.y = fmaf(cr, v.y, fmaf(ci, v.x, y.y));
+    };
+    mac(c01.x, c01.y, u0);
+    mac(c01.z, c01.w, u1);
+    mac(c23.x, c23.y, u2);
+    mac(c23.z, c23.w, u3);
+    mac(c45.x, c45.y, u4);
+    mac(c45.z, c45.w, u5);
+    return y;
+}
+
 template <typename R, bool ADJ, typename S = typename Tr<R>::c2>
 __device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op, const S* __restrict__ u,
                                                     long long n, Node p) {
     using C2 = typename Tr<R>::c2;
     using C4 = typename Tr<R>::c4;
-    const C2 un = widen<C2>(u[n]);
-    if (!ADJ && node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz)) return un;
-    const long long sy = op.nx, sz = (long long)op.nx * op.ny;
-    const long long off[6] = {-1, 1, -sy, sy, -sz, sz};
-    return k_row_from<R, ADJ>(op, p, op.rec[n], un, [&](int dir, C4& r, C2& uv) {
-        const long long m = n + off[dir];
-        r = op.rec[m];
-        uv = widen<C2>(u[m]);
-    });
+    if constexpr (sizeof(R) == 4) {
+        return k_row_cf(op, u, n, p);
+    } else {
+        const C2 un = widen<C2>(u[n]);
+        if (!ADJ && node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz)) return un;
+        const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+        const long long off[6] = {-1, 1, -sy, sy, -sz, sz};
+        return k_row_from<R, ADJ>(op, p, op.rec[n], un, [&](int dir, C4& r, C2& uv) {
+            const long long m = n + off[dir];
+            r = op.rec[m];
+            uv = widen<C2>(u[m]);
+        });
+    }
 }
 
 // z-marching application of the K rows (2.5-D blocking): a CTA owns a
