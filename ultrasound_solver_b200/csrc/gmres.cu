@@ -1195,6 +1195,277 @@ __global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState 
     if (threadIdx.x == 0) g.counter[b] = 0;
 }
 
+// The same product for bfloat16 storage on the tensor cores (mma.sync
+// m16n8k16, bf16 x bf16 -> fp32): out = In Coef with In = [U_old | C_old |
+// Krylov slots] (nodes x rows) and the 2K complex outputs as real columns.
+// A row of the product is a node; k runs over (input row, re/im), so a packed
+// {re, im} word of an input vector is one k pair of A. Each complex
+// coefficient c of output o gives four real columns: {Re, Im} of c v from the
+// bfloat16 part hi(c) and from the remainder lo(c) = c - hi(c) (16
+// significant bits of c); B fragments are built once per CTA in shared
+// memory in fragment order. A warp owns 16-node blocks; lane (g, c) loads the
+// words of nodes g and g+8 of input rows 8kb + c and 8kb + c + 4 and keeps
+// the accumulators of all K n-tiles (two outputs each).
+//   fragments: a = {A[g][2c..], A[g+8][2c..], A[g][2c+8..], A[g+8][2c+8..]},
+//   b = {B[2c..][g], B[2c+8..][g]}, d = {D[g][2c], D[g][2c+1], D[g+8][2c], D[g+8][2c+1]}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], unsigned a0, unsigned a1, unsigned a2,
+                                         unsigned a3, unsigned b0, unsigned b1) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ unsigned bf_pack(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return unsigned(__bfloat16_as_ushort(lo)) | (unsigned(__bfloat16_as_ushort(hi)) << 16);
+}
+static size_t combine_mma_smem(int k, int m) {
+    return sizeof(uint2) * size_t((k + m + 1 + 7) / 8) * k * 32;
+}
+template <int K>
+__global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, GState g) {
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE) return;
+    const int* cw = g.ctl + b * kCtl;
+    if (!cw[CW_COMBINE]) return;
+    const int m = g.m, skc = cw[CW_SRC_KC];
+    const int rows = skc + m + 1, nkb = (rows + 7) / 8;
+    extern __shared__ __align__(16) uint2 bfr[];  // [nkb][K][32]
+    __shared__ double sh[kThreads / 32][2 * K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g8 = lane >> 2, c4 = lane & 3;
+    const double2* coef = g.coef + (long long)b * (K + m + 1) * 2 * K;
+    // B fragment word of input row r, real column col (output col/4, part col%4)
+    auto bword = [&](int r, int col) -> unsigned {
+        if (r >= rows) return 0u;
+        const double2 c = coef[(long long)r * 2 * K + col / 4];
+        const bool lo = (col & 2) != 0, im = (col & 1) != 0;
+        __nv_bfloat16 cr = __double2bfloat16(c.x), ci = __double2bfloat16(c.y);
+        if (lo) {
+            cr = __double2bfloat16(c.x - double(__bfloat162float(cr)));
+            ci = __double2bfloat16(c.y - double(__bfloat162float(ci)));
+        }
+        // Re(c v) = c.re v.re - c.im v.im ; Im(c v) = c.im v.re + c.re v.im
+        return im ? bf_pack(ci, cr) : bf_pack(cr, __hneg(ci));
+    };
+    for (int q = threadIdx.x; q < nkb * K * 32; q += kThreads) {
+        const int ln = q % 32, nt = (q / 32) % K, kb = q / (32 * K);
+        const int gg = ln >> 2, cc = ln & 3, col = 8 * nt + gg;
+        bfr[q] = make_uint2(bword(8 * kb + cc, col), bword(8 * kb + cc + 4, col));
+    }
+    const long long sp = (cw[CW_SRC_PAIR] > 0 ? cw[CW_SRC_PAIR] : 0) * g.pstride + (long long)b * K * g.nv;
+    const long long dp = cw[CW_DST] * g.pstride + (long long)b * K * g.nv;
+    const unsigned* Uo = reinterpret_cast<const unsigned*>(static_cast<const bf2*>(g.Ubuf) + sp);
+    const unsigned* Co = reinterpret_cast<const unsigned*>(static_cast<const bf2*>(g.Cbuf) + sp);
+    unsigned* Un = reinterpret_cast<unsigned*>(static_cast<bf2*>(g.Ubuf) + dp);
+    unsigned* Cn = reinterpret_cast<unsigned*>(static_cast<bf2*>(g.Cbuf) + dp);
+    const unsigned* Vs = reinterpret_cast<const unsigned*>(V + cw[CW_SRC_VBUF] * g.vstride +
+                                                            (long long)b * (m + 1) * g.nv);
+    // input row r (rows past the last read row 0 and are zeroed)
+    auto row = [&](int r) {
+        r = r < rows ? r : 0;
+        return r < skc ? Uo + (long long)r * g.nv
+                       : (r < 2 * skc ? Co + (long long)(r - skc) * g.nv : Vs + (long long)(r - skc) * g.nv);
+    };
+    __syncthreads();
+    float nrm[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) nrm[i] = 0.f;
+    const long long nblk16 = (N + 15) / 16;
+    const long long wstride = (long long)gridDim.x * (kThreads / 32);
+    for (long long blk = (long long)blockIdx.x * (kThreads / 32) + warp; blk < nblk16; blk += wstride) {
+        const long long n0 = blk * 16 + g8, n1 = n0 + 8;
+        const long long l0 = n0 < N ? n0 : N - 1, l1 = n1 < N ? n1 : N - 1;
+        float acc[K][4];
+#pragma unroll
+        for (int nt = 0; nt < K; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll 2
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int ra = 8 * kb + c4, rb = ra + 4;
+            const unsigned* pa = row(ra);
+            const unsigned* pb = row(rb);
+            unsigned a0 = __ldg(pa + l0), a1 = __ldg(pa + l1), a2 = __ldg(pb + l0), a3 = __ldg(pb + l1);
+            if (ra >= rows) a0 = a1 = 0u;
+            if (rb >= rows) a2 = a3 = 0u;
+            const uint2* bq = bfr + (size_t)kb * K * 32 + lane;
+#pragma unroll
+            for (int nt = 0; nt < K; ++nt) {
+                const uint2 bb = bq[nt * 32];
+                mma_bf16(acc[nt], a0, a1, a2, a3, bb.x, bb.y);
+            }
+        }
+        // lanes c and c^1 hold the hi and lo parts of one output: add them;
+        // lane (g, 0) then has output 2nt, lane (g, 2) output 2nt+1
+#pragma unroll
+        for (int nt = 0; nt < K; ++nt) {
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[e] = acc[nt][e] + __shfl_xor_sync(0xffffffffu, acc[nt][e], 1);
+            if ((c4 & 1) == 0) {
+                const int o = 2 * nt + (c4 >> 1);
+                const bf2 w0 = __floats2bfloat162_rn(v[0], v[1]);
+                const bf2 w1 = __floats2bfloat162_rn(v[2], v[3]);
+                unsigned* dst = o < K ? Un + (long long)o * g.nv : Cn + (long long)(o - K) * g.nv;
+                if (n0 < N) dst[n0] = *reinterpret_cast<const unsigned*>(&w0);
+                if (n1 < N) dst[n1] = *reinterpret_cast<const unsigned*>(&w1);
+                if (o < K) {
+                    const float2 f0 = to_f(w0), f1 = to_f(w1);
+                    float add = 0.f;
+                    if (n0 < N) add += f0.x * f0.x + f0.y * f0.y;
+                    if (n1 < N) add += f1.x * f1.x + f1.y * f1.y;
+                    nrm[nt] += add;
+                }
+            }
+        }
+    }
+    // ||U'_o||^2: lane (g, c) with c even holds output 2nt + c/2 in nrm[nt]
+#pragma unroll
+    for (int nt = 0; nt < K; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int o = 2 * nt + h;
+            const double t = warp_sum((c4 & 1) == 0 && (c4 >> 1) == h ? double(nrm[nt]) : 0.0);
+            if (lane == 0 && o < K) sh[warp][o] = t;
+        }
+    __syncthreads();
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+    for (int o = threadIdx.x; o < K; o += kThreads) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) t += sh[w][o];
+        part[o] = make_double2(t, 0.0);
+    }
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    for (int i = threadIdx.x; i < K; i += kThreads) {
+        double t = 0.0;
+        const double2* pq = g.partial + (long long)b * g.nblk * g.ps + i;
+        for (int c = 0; c < int(gridDim.x); ++c) t += ld_cg(pq + (long long)c * g.ps).x;
+        g.dU[((long long)cw[CW_DST] * gridDim.y + b) * K + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
+    }
+    if (threadIdx.x == 0) g.counter[b] = 0;
+}
+
+// bd = Vhat^H Ut for bfloat16 storage on the tensor cores: D = A B with A
+// rows = the slots s <= m of Vhat (16 per row tile), k = (node, re/im), and
+// B columns {re, im} -> Re, {im, -re} -> Im of <Vhat_s, U_i> (exact bf16
+// words, no split). Lane (g, c) loads the 16-byte unit at node 16j + 4c of
+// slots s0 + g and s0 + g + 8 and of U_i, i = 4nt + g/2, and feeds its four
+// words to two products. Global warp w owns row tile w % RT and every
+// (W / RT)-th 16-node block; fp32 sums are moved to FP64 every 16 blocks and
+// the warps of a CTA are added in a fixed order.
+static size_t bdots_mma_smem(int k, int m) {
+    return sizeof(double2) * (size_t(kThreads / 32) * 16 + size_t(m + 1)) * k;
+}
+template <int K>
+__global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GState g) {
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
+    const CycleBasis<bf2> cb = cycle_basis(V, g, b);
+    const int m = g.m;
+    if (cb.kc != K) return;  // recycled cycles use all K vectors
+    if (!g.ctl[b * kCtl + CW_HARVEST]) return;
+    constexpr int NT = (2 * K + 7) / 8;
+    const int RT = (m + 16) / 16;  // row tiles of 16 slots covering 0..m
+    extern __shared__ __align__(16) double2 wtab[];  // [warps][16][K], then the CTA's [m+1][K]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g8 = lane >> 2, c4 = lane & 3;
+    constexpr int nw = kThreads / 32;
+
+    const long long W = (long long)gridDim.x * nw, wg = (long long)blockIdx.x * nw + warp;
+    const int rt = int(wg % RT);
+    const long long wstride = W / RT;
+    const int sa = 16 * rt + g8, sb = sa + 8;
+    auto slot_ptr = [&](int sl) {
+        sl = sl <= m ? sl : 0;
+        return reinterpret_cast<const uint4*>((sl < K ? cb.C : cb.V) + (long long)sl * g.nv);
+    };
+    const uint4* pa = slot_ptr(sa);
+    const uint4* pb = slot_ptr(sb);
+    const uint4* pu[NT];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        const int i = 4 * nt + g8 / 2;
+        pu[nt] = reinterpret_cast<const uint4*>(cb.U + (long long)(i < K ? i : 0) * g.nv);
+    }
+    double2 tot[NT][2];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) tot[nt][0] = tot[nt][1] = make_double2(0.0, 0.0);
+    const long long nb16 = (N + 15) / 16, lastu = (N + 3) / 4 - 1;
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    if (wg < wstride * RT) {
+        long long blk = wg / RT;
+        while (blk < nb16) {
+            float d[NT][4];
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
+            for (int r = 0; r < 16 && blk < nb16; ++r, blk += wstride) {
+                const long long uq = 4 * blk + c4;
+                const long long uc = uq < lastu ? uq : lastu;
+                uint4 va = __ldg(pa + uc), vb = __ldg(pb + uc);
+                if (!(sa <= m && uq <= lastu)) va = zero;
+                if (!(sb <= m && uq <= lastu)) vb = zero;
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+                    uint4 w = __ldg(pu[nt] + uc);
+                    if (!(4 * nt + g8 / 2 < K && uq <= lastu)) w = zero;
+                    if (g8 & 1) {
+                        w.x = (w.x >> 16) | ((w.x << 16) ^ 0x80000000u);
+                        w.y = (w.y >> 16) | ((w.y << 16) ^ 0x80000000u);
+                        w.z = (w.z >> 16) | ((w.z << 16) ^ 0x80000000u);
+                        w.w = (w.w >> 16) | ((w.w << 16) ^ 0x80000000u);
+                    }
+                    mma_bf16(d[nt], va.x, vb.x, va.y, vb.y, w.x, w.y);
+                    mma_bf16(d[nt], va.z, vb.z, va.w, vb.w, w.z, w.w);
+                }
+            }
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                tot[nt][0] = cadd(tot[nt][0], make_double2(d[nt][0], d[nt][1]));
+                tot[nt][1] = cadd(tot[nt][1], make_double2(d[nt][2], d[nt][3]));
+            }
+        }
+    }
+    // lane (g, c): <slot sa|sb, U_{4nt+c}> in tot[nt][0|1]
+    double2* mine = wtab + (size_t)warp * 16 * K;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        const int i = 4 * nt + c4;
+        if (i < K) {
+            mine[g8 * K + i] = tot[nt][0];
+            mine[(g8 + 8) * K + i] = tot[nt][1];
+        }
+    }
+    __syncthreads();
+    // CTA sums in warp order: slot sl comes from the warps whose row tile is sl/16
+    double2* tab = wtab + (size_t)nw * 16 * K;
+    for (int q = threadIdx.x; q < (m + 1) * K; q += kThreads) {
+        const int sl = q / K, i = q % K;
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = 0; w < nw; ++w)
+            if (int(((long long)blockIdx.x * nw + w) % RT) == sl / 16)
+                t = cadd(t, wtab[(size_t)w * 16 * K + (sl % 16) * K + i]);
+        tab[q] = t;
+    }
+    __syncthreads();
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+    for (int q = threadIdx.x; q < (m + 1) * K; q += kThreads) part[q] = tab[q];
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    const double* dd = g.dU + ((long long)cb.pair * gridDim.y + b) * g.kr;
+    double* out = g.hb + (long long)b * g.hb_len + hb_bd(m);
+    for (int q = threadIdx.x; q < (m + 1) * K; q += kThreads) {
+        double re = 0.0, im = 0.0;
+        const double2* pq = g.partial + (long long)b * g.nblk * g.ps + q;
+        for (int c = 0; c < int(gridDim.x); ++c) {
+            const double2 v = ld_cg(pq + (long long)c * g.ps);
+            re += v.x;
+            im += v.y;
+        }
+        const int sl = q / K, i = q % K;
+        const double sc = (sl < K ? 1.0 : g.sigma[b * (m + 1) + sl]) * dd[i];
+        out[2 * (sl + (m + 1) * i)] = re * sc;
+        out[2 * (sl + (m + 1) * i) + 1] = im * sc;
+    }
+    if (threadIdx.x == 0) g.counter[b] = 0;
+}
+
 // ------------------------------------------------------------ final gates (fp64)
 // iterative_solver.py:70-79: ||R(OP x) - Rb|| / ||Rb|| and
 // max |OP x - b| / max(|OP||x| + |b|, 1e-30), plus a finiteness check.
@@ -1269,6 +1540,8 @@ static cudaStream_t capture_stream() {
 
 // The recycled-space kernels are instantiated for every k = 1..kMaxRecycle.
 template <typename S, int K> const void* recycle_kernel_k(bool combine) {
+    if constexpr (std::is_same<S, bf2>::value)
+        return combine ? (const void*)k_combine_mma<K> : (const void*)k_bdots_mma<K>;
     return combine ? (const void*)k_combine<S, K> : (const void*)k_bdots<S, K>;
 }
 template <typename S> const void* recycle_kernel(int k, bool combine) {
@@ -1416,8 +1689,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     const void* fn_comb = nullptr;
     if (kr > 0) {
         using T = typename Wide<S>::T;
-        bd_smem = sizeof(T) * size_t(kr) * kBdTile + sizeof(double2) * size_t(g.m + 1) * kr;
-        comb_smem = sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
+        bd_smem = std::is_same<S, bf2>::value
+                      ? bdots_mma_smem(kr, g.m)
+                      : sizeof(T) * size_t(kr) * kBdTile + sizeof(double2) * size_t(g.m + 1) * kr;
+        comb_smem = std::is_same<S, bf2>::value ? combine_mma_smem(kr, g.m)
+                                                : sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
         fn_bdots = recycle_kernel<S>(kr, false);
         fn_comb = recycle_kernel<S>(kr, true);
         if (!fn_bdots || !fn_comb) return USV_ERR_ARG;
@@ -1475,6 +1751,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     // only runs in recycled cycles (1) or with a new pair (2), so that the
     // empty launches of a cycle count no bytes
     std::vector<int> fam_step, fam_need;
+    std::vector<double> fam_shared;  // bytes read once per launch for all RHS
     auto mark = [&](cudaStream_t st, int idx, bool capturing) {
         if (!prof) return cudaSuccess;
         return capturing ? cudaEventRecordWithFlags(ev[idx], st, cudaEventRecordExternal)
@@ -1486,6 +1763,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         fam_bytes.clear();
         fam_step.clear();
         fam_need.clear();
+        fam_shared.clear();
         USV_CUDA_TRY(mark(st, k++, capturing));
         if (kr > 0) {
             // new pair (when the host supplied coefficients), FP64 residual into
@@ -1499,13 +1777,15 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             }
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(6);
-            fam_bytes.push_back(nn * vb * (2.0 * g.m + 2 * kr + 1));
+            fam_bytes.push_back(nn * vb * (g.m + 1.0 + 3 * kr));  // read U, C, slots kc..m; write U', C'
+            fam_shared.push_back(0.0);
             fam_step.push_back(-1);
             fam_need.push_back(2);
             k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
             fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
+            fam_shared.push_back(0.0);
             fam_step.push_back(-1);
             fam_need.push_back(0);
             launch_dots(st, 0, 1);
@@ -1513,6 +1793,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(7);
             fam_bytes.push_back(nn * vb * (2.0 * kr + 3));
+            fam_shared.push_back(0.0);
             fam_step.push_back(-1);
             fam_need.push_back(1);
         }
@@ -1520,15 +1801,18 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             launch_dots(st, j, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
-            // read u_0..u_j (u_j also feeds the stencil) + the row coefficients
-            // (complex64: 48 B) or node record (complex128: 32 B), write w
-            fam_bytes.push_back(nn * (vb * (j + 2) + (sizeof(R) == 4 ? 48.0 : 32.0)));
+            // per RHS: read u_0..u_j (u_j also feeds the stencil), write w; per
+            // launch: the row coefficients (complex64: 48 B) or node records
+            // (complex128: 32 B), the same for every RHS of the batch
+            fam_bytes.push_back(nn * vb * (j + 2));
+            fam_shared.push_back(nn * (sizeof(R) == 4 ? 48.0 : 32.0));
             fam_step.push_back(j);
             fam_need.push_back(0);
             k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j, 0);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(1);
             fam_bytes.push_back(nn * vb * (j + 3));
+            fam_shared.push_back(0.0);
             fam_step.push_back(j);
             fam_need.push_back(0);
         }
@@ -1536,12 +1820,14 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(2);
         fam_bytes.push_back(0.0);
+        fam_shared.push_back(0.0);
         fam_step.push_back(-1);
         fam_need.push_back(0);
         k_update<S><<<grid_upd, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(3);
         fam_bytes.push_back(nn * (vb * g.m + 2 * sizeof(double2) + sizeof(double4)));
+        fam_shared.push_back(0.0);
         fam_step.push_back(-1);
         fam_need.push_back(0);
         if (kr > 0) {
@@ -1556,6 +1842,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(7);
             fam_bytes.push_back(nn * vb * (g.m + 1.0 + kr));
+            fam_shared.push_back(0.0);
             fam_step.push_back(-1);
             fam_need.push_back(3);
             USV_CUDA_TRY(cudaMemcpyAsync(hb_pin.p, ws + L.hb, hb_bytes, cudaMemcpyDeviceToHost, st));
@@ -1564,6 +1851,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
             fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
+            fam_shared.push_back(0.0);
             fam_step.push_back(-1);
             fam_need.push_back(0);
         }
@@ -1583,7 +1871,8 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
                               (fam_need[i] == 1 && meas_kc == 0) ||
                               (fam_need[i] == 2 && !meas_combine) ||
                               (fam_need[i] == 3 && (meas_kc == 0 || !meas_harvest));
-            if (!idle) prof->bytes[fam[i]] += fam_bytes[i] * active_counts[0];
+            if (!idle && active_counts[0] > 0)
+                prof->bytes[fam[i]] += fam_bytes[i] * active_counts[0] + fam_shared[i];
         }
         return USV_OK;
     };
