@@ -74,6 +74,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient timing")
+    ap.add_argument("--no-stencil", action="store_true", help="skip the stencil-only timing")
     ap.add_argument("--cpu-iters", type=int, default=20)
     return ap.parse_args(argv)
 
@@ -222,12 +223,13 @@ def run_ours(args):
     it.backward_error_tol = 1e-4
     stream = torch.cuda.current_stream()
 
-    def configure(precision, profile=False):
-        it.precision, it.profile = precision, profile
+    def configure(precision, profile=False, its=None):
+        its = it if its is None else its
+        its.precision, its.profile = precision, profile
         if precision == "fp64":
-            it.restart, it.recycle = args.fp64_restart, 0
+            its.restart, its.recycle = args.fp64_restart, 0
         else:
-            it.restart, it.recycle, it.recycle_every = args.restart, args.recycle, args.recycle_every
+            its.restart, its.recycle, its.recycle_every = args.restart, args.recycle, args.recycle_every
 
     def solve(precision, profile=False, b=None):
         configure(precision, profile)
@@ -294,6 +296,58 @@ def run_ours(args):
                                         if v["ms"] > 0 and v["bytes"] > 0 else None}
                                     for k, v in prof_tot.items()}}
 
+    # the stencil alone: usv_operator_apply of the complex64 K rows and of the
+    # FP64 A rows on the batch, each launch timed with CUDA events after an L2
+    # flush; algorithmic bytes per launch: the per-node operator data once
+    # (complex64 row coefficients 48 B; FP64 node record + diagonal 48 B) plus
+    # x and y of every RHS
+    if not args.no_stencil:
+        from ultrasound_solver_b200 import _native as N
+        op = solver.operator
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        nn = op.n
+
+        import ctypes
+
+        def time_apply(x, variant, precision, reps=20):
+            # back-to-back launches through the C-ABI (the batch's operator data
+            # and vectors, >= 234 MB, exceed the 126 MB L2), after an L2 flush
+            y = torch.empty_like(x)
+            lib, sh = N.load(), N.stream_handle(torch, x.device)
+
+            def launch():
+                N.check(lib.usv_operator_apply(ctypes.byref(op.scene), N.ptr(op.buffer), variant,
+                                               precision, N.ptr(x), N.ptr(y), x.shape[0], op.n,
+                                               sh), "apply")
+            for _ in range(3):
+                launch()
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                launch()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return max_over_ranks(e0.elapsed_time(e1) / reps, world)
+
+        x64 = rhs.to(torch.complex64).contiguous()
+        ms_k = time_apply(x64, N.APPLY_K, N.PREC_MIXED)
+        bytes_k = nn * (48.0 + args.batch * 16.0)
+        ms_a = time_apply(rhs.contiguous(), N.APPLY_A, N.PREC_FP64)
+        bytes_a = nn * (48.0 + args.batch * 32.0)
+        peak, peak_kind = measured_peak()
+        out["stencil"] = {
+            "kernel": f"k_apply_kc (complex64 K rows), {args.batch} RHS per launch",
+            "achieved": bytes_k / (ms_k / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
+            "frac": bytes_k / (ms_k / 1e3) / 1e9 / peak, "us_per_launch": 1000.0 * ms_k,
+            "bytes_per_launch": bytes_k, "l2": "inputs larger than L2 (20 launches back to back)",
+            "fp64_A": {"kernel": f"k_apply_fp64 (complex128 A rows), {args.batch} RHS per launch",
+                       "achieved": bytes_a / (ms_a / 1e3) / 1e9,
+                       "frac": bytes_a / (ms_a / 1e3) / 1e9 / peak,
+                       "us_per_launch": 1000.0 * ms_a, "bytes_per_launch": bytes_a}}
+        del flush
+
     # plain FP64 GMRES of the same stencil (comparator) + parity of the two fields
     fp64_iters = None
     if not args.no_fp64:
@@ -331,21 +385,27 @@ def run_ours(args):
 
     # adjoint gradient: forward solve + A^H solve + phase VJP behind torch.autograd,
     # in the mixed path and (unless --no-fp64) with the plain FP64 GMRES
+    # on the adjoint workload's scene: the same medium with a 16x16 array
     if not args.no_adjoint:
         from ultrasound_solver_b200.autograd import loss_of_field, phase_field
         from ultrasound_solver_b200.losses import ContrastRatioLoss
-        centre = (args.grid - 1) * solver.cfg.domain.dx / 2
-        loss = ContrastRatioLoss(solver.cfg, (centre, centre, 0.080), 0.006, 0.010)
+        asolver = W.build_solver(W.config3(n=args.grid), seed=0)
+        asolver.assemble_matrix()
+        asolver.set_phases(rng.uniform(0, 2 * np.pi, asolver.transducers.num_transducers))
+        ait = asolver.iterative_solver
+        ait.rtol, ait.maxiter, ait.backward_error_tol = args.rtol, args.maxiter, 1e-4
+        centre = (args.grid - 1) * asolver.cfg.domain.dx / 2
+        loss = ContrastRatioLoss(asolver.cfg, (centre, centre, 0.080), 0.006, 0.010)
 
         def grad_once(precision):
-            configure(precision)
-            ph = torch.tensor(solver.transducers.phases, dtype=torch.float64, device="cuda",
+            configure(precision, its=ait)
+            ph = torch.tensor(asolver.transducers.phases, dtype=torch.float64, device="cuda",
                               requires_grad=True)
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            L = loss_of_field(phase_field(ph, solver), loss)
+            L = loss_of_field(phase_field(ph, asolver), loss)
             L.backward()
             e1.record(stream)
             torch.cuda.synchronize()
@@ -354,6 +414,8 @@ def run_ours(args):
         ms_grad, grad = grad_once(args.precision)
         out["adjoint_grad"] = {"value": world * 1000.0 / ms_grad, "unit": "adjoint grads/s",
                                "ms_per_grad": ms_grad,
+                               "scene": f"{args.grid}^3 random medium and sphere as above with a "
+                                        f"{asolver.transducers.num_transducers}-element (16x16) array",
                                "loss": "-|u_t|^2 / mean_shell |u|^2 (target 80 mm above the array)",
                                "grad_norm": float(torch.linalg.norm(grad).item())}
         if not args.no_fp64:

@@ -250,9 +250,91 @@ __global__ void __launch_bounds__(256) k_apply_k(OpView<R> op, const typename Tr
     }
 }
 
+// y = K x for complex64 from the precomputed row coefficients: one thread per
+// node reads the node's coefficients once and applies them to every
+// right-hand side (nrhs vectors at stride ld), so a batch reads the operator
+// data once.
+__global__ void __launch_bounds__(256, 4) k_apply_kc(OpView<float> op, const float2* __restrict__ x,
+                                                  float2* __restrict__ y, long long ld, Step step,
+                                                  int nrhs) {
+    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    Node p = decode(n, op.nx, op.ny);
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+    for (; n < op.n; n += (long long)gridDim.x * blockDim.x) {
+        const float4* cf = op.cf + 3 * n;
+        const float4 c01 = __ldg(cf), c23 = __ldg(cf + 1), c45 = __ldg(cf + 2);
+        const long long i0 = p.i > 0 ? n - 1 : n, i1 = p.i < op.nx - 1 ? n + 1 : n;
+        const long long i2 = p.j > 0 ? n - sy : n, i3 = p.j < op.ny - 1 ? n + sy : n;
+        const long long i4 = p.k > 0 ? n - sz : n, i5 = p.k < op.nz - 1 ? n + sz : n;
+#pragma unroll 2
+        for (int b = 0; b < nrhs; ++b) {
+            const float2* xb = x + b * ld;
+            float2 v = __ldg(xb + n);
+            auto mac = [&](float cr, float ci, float2 u) {
+                v.x = fmaf(cr, u.x, fmaf(-ci, u.y, v.x));
+                v.y = fmaf(cr, u.y, fmaf(ci, u.x, v.y));
+            };
+            mac(c01.x, c01.y, __ldg(xb + i0));
+            mac(c01.z, c01.w, __ldg(xb + i1));
+            mac(c23.x, c23.y, __ldg(xb + i2));
+            mac(c23.z, c23.w, __ldg(xb + i3));
+            mac(c45.x, c45.y, __ldg(xb + i4));
+            mac(c45.z, c45.w, __ldg(xb + i5));
+            y[b * ld + n] = v;
+        }
+        advance(p, step, op.nx, op.ny);
+    }
+}
+
+// The same for batches of up to 8 right-hand sides on a 3-D grid, so that no
+// thread divides: a CTA of 32 x 8 threads covers 32 nodes along x of a few
+// rows j of plane k. The R right-hand sides (nrhs rounded up to a power of
+// two) are split into G = R / NB groups of NB; a thread applies its node's
+// coefficients (loaded once) to the NB vectors b = g, g + G, ..., and each
+// warp holds 32 consecutive nodes (coalesced loads and stores); the G warps
+// of a row share its coefficient loads through L1.
+template <int R, int NB>
+__global__ void __launch_bounds__(256) k_apply_kc_rhs(OpView<float> op, const float2* __restrict__ x,
+                                                      float2* __restrict__ y, long long ld, int nrhs) {
+    constexpr int G = R / NB, kRows = 8 / G;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int g = threadIdx.y % G;
+    const int j = blockIdx.y * kRows + threadIdx.y / G;
+    const int k = blockIdx.z;
+    if (i >= op.nx || j >= op.ny || g >= nrhs) return;
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+    const long long n = i + sy * j + sz * k;
+    const float4* cf = op.cf + 3 * n;
+    const float4 c01 = __ldg(cf), c23 = __ldg(cf + 1), c45 = __ldg(cf + 2);
+    const long long o0 = i > 0 ? -1 : 0, o1 = i < op.nx - 1 ? 1 : 0;
+    const long long o2 = j > 0 ? -sy : 0, o3 = j < op.ny - 1 ? sy : 0;
+    const long long o4 = k > 0 ? -sz : 0, o5 = k < op.nz - 1 ? sz : 0;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const int b = g + G * q;
+        if (b < nrhs) {
+            const float2* xb = x + b * ld + n;
+            float2 v = __ldg(xb);
+            const float2 u0 = __ldg(xb + o0), u1 = __ldg(xb + o1), u2 = __ldg(xb + o2);
+            const float2 u3 = __ldg(xb + o3), u4 = __ldg(xb + o4), u5 = __ldg(xb + o5);
+            auto mac = [&](float cr, float ci, float2 u) {
+                v.x = fmaf(cr, u.x, fmaf(-ci, u.y, v.x));
+                v.y = fmaf(cr, u.y, fmaf(ci, u.x, v.y));
+            };
+            mac(c01.x, c01.y, u0);
+            mac(c01.z, c01.w, u1);
+            mac(c23.x, c23.y, u2);
+            mac(c23.z, c23.w, u3);
+            mac(c45.x, c45.y, u4);
+            mac(c45.z, c45.w, u5);
+            y[b * ld + n] = v;
+        }
+    }
+}
+
 // y = K x through the z-marching tile kernel (usv_internal.cuh: zmarch_rows).
 // usv_operator_apply K / K^H: z-marching kernel for complex128 (74 vs 97 us at
-// 128^3), the direct kernel for complex64 (35 vs 40 us).
+// 128^3); complex64 uses the coefficient rows (k_apply_kc_rhs / k_apply_kc).
 constexpr bool kZMarch64 = true, kZMarch32 = false;
 template <typename R, bool ADJ>
 __global__ void __launch_bounds__(kZTX * kZTY) k_apply_k25(OpView<R> op, const typename Tr<R>::c2* x,
@@ -442,9 +524,20 @@ int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant, 
                 if (kZMarch32) {
                     if (adj) k_apply_k25<float, true><<<g25, kZTX * kZTY, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, zseg);
                     else k_apply_k25<float, false><<<g25, kZTX * kZTY, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, zseg);
+                } else if (nrhs <= 8 && s.nz <= 65535) {
+                    const float2* xf = (const float2*)x;
+                    float2* yf = (float2*)y;
+                    const int r = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : 8;
+                    const int rows = 8 / (r == 1 ? 1 : r / 2);  // rows of a CTA: 8 / groups
+                    const dim3 g3((s.nx + 31) / 32, (s.ny + rows - 1) / rows, s.nz);
+                    const dim3 b3(32, 8);
+                    if (r == 1) k_apply_kc_rhs<1, 1><<<g3, b3, 0, strm>>>(v, xf, yf, ld, nrhs);
+                    else if (r == 2) k_apply_kc_rhs<2, 2><<<g3, b3, 0, strm>>>(v, xf, yf, ld, nrhs);
+                    else if (r == 4) k_apply_kc_rhs<4, 2><<<g3, b3, 0, strm>>>(v, xf, yf, ld, nrhs);
+                    else k_apply_kc_rhs<8, 2><<<g3, b3, 0, strm>>>(v, xf, yf, ld, nrhs);
                 } else {
-                    if (adj) k_apply_k<float, true><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, step);
-                    else k_apply_k<float, false><<<grid, 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, step);
+                    k_apply_kc<<<dim3(grid.x), 256, 0, strm>>>(v, (const float2*)x, (float2*)y, ld,
+                                                               step, nrhs);
                 }
             } else {
                 return USV_ERR_ARG;

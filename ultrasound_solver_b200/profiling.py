@@ -13,7 +13,7 @@ k_dots|k_orth 2(m+1) times (the projection pair, then steps j = 0..m-1, the
 steps j < k returning at once): skipping 2(m+1)c + 2 + 2j lands on step j of
 cycle c >= 2. One launch covers all --batch right-hand sides (random
 transducer phases, as in the bench). `stencil` applies the K and A operators
-a few times. Both exit 0 without converging anything.
+a few times (to --batch vectors in one launch). Both exit 0 without converging anything.
 """
 from __future__ import annotations
 
@@ -57,7 +57,8 @@ def main(argv=None):
         print("cycle", it.last_stats[0])
     else:
         op = solver.operator
-        x64 = torch.randn(op.n, dtype=torch.complex128, device="cuda")
+        x64 = torch.randn((args.batch, op.n) if args.batch > 1 else op.n, dtype=torch.complex128,
+                          device="cuda")
         for _ in range(3):
             op.apply(x64.to(torch.complex64), N.APPLY_K, N.PREC_MIXED)
             op.apply(x64, N.APPLY_K, N.PREC_FP64)
