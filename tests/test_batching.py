@@ -84,3 +84,27 @@ def test_concurrent_scenes_match_sequential():
     for g, x in zip(gs, xs):
         want = g["x_direct"]
         assert rel(x.cpu().numpy(), want) <= 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nrhs", [3, 4, 9])
+def test_mixed_apply_on_an_uneven_grid(nrhs):
+    """Complex64 K on a grid whose x edge is not a multiple of the 32-node warp
+    span (an uneven-batch scene) matches the FP64 rows per column."""
+    import torch
+    from tests.helpers import rel
+    from ultrasound_solver_b200 import _native as N
+    from ultrasound_solver_b200 import workloads as W
+    cfg = W.config2_scene_batch(count=1, seed=5, sizes=(48, 80, 112))[0]
+    s = W.build_solver(cfg, seed=0)
+    s.assemble_matrix()
+    op = s.operator
+    assert op.shape[0] % 32 != 0 or op.shape[1] % 8 != 0
+    rng = np.random.default_rng(nrhs)
+    x = torch.from_numpy(rng.standard_normal((nrhs, op.n)) + 1j * rng.standard_normal((nrhs, op.n)))
+    x = x.cuda()
+    for var in (N.APPLY_K, N.APPLY_KH):
+        got = op.apply(x.to(torch.complex64), var, N.PREC_MIXED).cpu().numpy()
+        want = op.apply(x, var, N.PREC_FP64).cpu().numpy()
+        for b in range(nrhs):
+            assert rel(got[b], want[b]) < 2e-6
