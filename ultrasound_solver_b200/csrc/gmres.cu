@@ -766,6 +766,17 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     if (threadIdx.x == 0) g.counter[b] = 0;
 }
 
+// d = a * b + c on two fp32 lanes at once (PTX fma.rn.f32x2, sm_100)
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const unsigned long long*>(&a)),
+          "l"(*reinterpret_cast<const unsigned long long*>(&b)),
+          "l"(*reinterpret_cast<const unsigned long long*>(&c)));
+    return *reinterpret_cast<const float2*>(&d);
+}
+
 // ------------------------------------------------------------ Arnoldi: orthogonalise + norm
 // proj = 1 (recycled cycles): r -= sum_t alpha_t C_t on the cycle's first
 // residual (slot kc), then beta = ||r|| starts the Krylov part of the cycle.
@@ -807,12 +818,34 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
             if (e < len) ld_pair(w + e, u[k][0], u[k][1]);
             else u[k][0] = u[k][1] = cmake<M2>(0.0, 0.0);
         }
-        stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
-                         [&](int t, int k, int c, M2 vv) {
-            const M2 h = hm[t];
-            u[k][c].x -= h.x * vv.x - h.y * vv.y;
-            u[k][c].y -= h.x * vv.y + h.y * vv.x;
-        });
+        if constexpr (std::is_same<C2, bf2>::value) {
+            // packed fp32x2 FMAs: u = (re, im) -= h.re (v.re, v.im) and a second
+            // pair q += h.im (-v.re, v.im) holding (Im, Re) terms, so neither
+            // needs the swapped pair (v.im, v.re): two FMAs per complex product
+            float2 q[kPairs][2];
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k) q[k][0] = q[k][1] = make_float2(0.f, 0.f);
+            stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
+                             [&](int t, int k, int c, M2 vv) {
+                const M2 h = hm[t];
+                u[k][c] = ffma2(vv, make_float2(-h.x, -h.x), u[k][c]);
+                q[k][c] = ffma2(vv, make_float2(-h.y, h.y), q[k][c]);
+            });
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    u[k][c].x += q[k][c].y;
+                    u[k][c].y += q[k][c].x;
+                }
+        } else {
+            stream_basis<C2>(stg, cb.C + n0, cb.V + n0, cb.kc, g.nv, j, len, false,
+                             [&](int t, int k, int c, M2 vv) {
+                const M2 h = hm[t];
+                u[k][c].x -= h.x * vv.x - h.y * vv.y;
+                u[k][c].y -= h.x * vv.y + h.y * vv.x;
+            });
+        }
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
             const int e = pair_node<C2>(k);
