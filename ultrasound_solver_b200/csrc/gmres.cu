@@ -606,7 +606,10 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     }
     // w of the chunk in shared memory, widened once for complex64 (FP64 dots)
     using YS = typename std::conditional<std::is_same<C2, float2>::value, double2, C2>::type;
-    __shared__ __align__(16) YS ys[kChunk];
+    // bfloat16: two chunks per phase (half the barriers, twice the loads in
+    // flight per phase)
+    constexpr int DC = std::is_same<C2, bf2>::value ? 2 * kChunk : kChunk;
+    __shared__ __align__(16) YS ys[DC];
     __shared__ double2 segsum[USV_MAX_RESTART + 2 > NT / 16 ? USV_MAX_RESTART + 2 : NT / 16];
     const long long N = op.n;
     const C2* uj = cb.V + (long long)j * g.nv;
@@ -621,15 +624,16 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     // segsum in chunk order
     for (int task = threadIdx.x; task < tasks_t * segs; task += NT)
         segsum[task] = make_double2(0.0, 0.0);
-    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
-        const long long n0 = (long long)ch * kChunk;
-        const int len = int(min((long long)kChunk, N - n0));
+    const int nphase = int((N + DC - 1) / DC);
+    for (int ch = blockIdx.x; ch < nphase; ch += gridDim.x) {
+        const long long n0 = (long long)ch * DC;
+        const int len = int(min((long long)DC, N - n0));
         __syncthreads();  // the previous chunk's dots are done with ys
         if (mode == 0) {
             Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
             constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
 #pragma unroll(kStencilUnroll)
-            for (int e = threadIdx.x; e < kChunk; e += NT) {
+            for (int e = threadIdx.x; e < DC; e += NT) {
                 C2 y = from_d<C2>(make_double2(0.0, 0.0));
                 if (e < len) {
                     const long long n = n0 + e;
@@ -640,7 +644,7 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
                 advance(p, step, op.nx, op.ny);
             }
         } else {
-            for (int e = threadIdx.x; e < kChunk; e += NT)
+            for (int e = threadIdx.x; e < DC; e += NT)
                 ys[e] = as_ys<YS>(e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0)));
         }
         __syncthreads();
