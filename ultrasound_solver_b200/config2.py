@@ -37,8 +37,8 @@ def main(argv=None):
     ap.add_argument("--columns", type=int, default=256)
     ap.add_argument("--scenes", type=int, default=32)
     ap.add_argument("--precision", default="bf16")
-    ap.add_argument("--restart", type=int, default=40)
-    ap.add_argument("--recycle", type=int, default=10)
+    ap.add_argument("--restart", type=int, default=36)
+    ap.add_argument("--recycle", type=int, default=8)
     ap.add_argument("--recycle-every", type=int, default=2)
     ap.add_argument("--rtol", type=float, default=1e-9)
     ap.add_argument("--maxiter", type=int, default=80000)
