@@ -299,8 +299,8 @@ def run_ours(args):
     # the stencil alone: usv_operator_apply of the complex64 K rows and of the
     # FP64 A rows on the batch, each launch timed with CUDA events after an L2
     # flush; algorithmic bytes per launch: the per-node operator data once
-    # (complex64 row coefficients 48 B; FP64 node record + diagonal 48 B) plus
-    # x and y of every RHS
+    # (complex64 row coefficients 48 B; FP64 diagonal + six edge coefficients
+    # 112 B) plus x and y of every RHS
     if not args.no_stencil:
         from ultrasound_solver_b200 import _native as N
         op = solver.operator
@@ -335,7 +335,7 @@ def run_ours(args):
         ms_k = time_apply(x64, N.APPLY_K, N.PREC_MIXED)
         bytes_k = nn * (48.0 + args.batch * 16.0)
         ms_a = time_apply(rhs.contiguous(), N.APPLY_A, N.PREC_FP64)
-        bytes_a = nn * (48.0 + args.batch * 32.0)
+        bytes_a = nn * (112.0 + args.batch * 32.0)
         peak, peak_kind = measured_peak()
         out["stencil"] = {
             "kernel": f"k_apply_kc (complex64 K rows), {args.batch} RHS per launch",

@@ -1821,8 +1821,10 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
-            fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
-            fam_shared.push_back(0.0);
+            // per RHS: x, b, the stored residual; per launch: node record (R),
+            // diagonal and the six FP64 edge coefficients
+            fam_bytes.push_back(nn * (2 * sizeof(double2) + vb));
+            fam_shared.push_back(nn * (sizeof(double4) + 7 * sizeof(double2)));
             fam_step.push_back(-1);
             fam_need.push_back(0);
             launch_dots(st, 0, 1);
@@ -1887,8 +1889,10 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
-            fam_bytes.push_back(nn * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2) + vb));
-            fam_shared.push_back(0.0);
+            // per RHS: x, b, the stored residual; per launch: node record (R),
+            // diagonal and the six FP64 edge coefficients
+            fam_bytes.push_back(nn * (2 * sizeof(double2) + vb));
+            fam_shared.push_back(nn * (sizeof(double4) + 7 * sizeof(double2)));
             fam_step.push_back(-1);
             fam_need.push_back(0);
         }

@@ -186,6 +186,31 @@ __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
     }
 }
 
+// FP64 edge coefficients of A for the FP64 rows (usv_internal.cuh: a_row):
+// e_nd = F_d 2/(rho_n + rho_d), F_d the face product of the direction tables,
+// by the same expressions a row used to evaluate on the fly (bit-identical);
+// zero where the neighbour is missing.
+__global__ void __launch_bounds__(256) k_edges(OpView<double> op, double2* e64) {
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
+         n += (long long)gridDim.x * blockDim.x) {
+        const Node p = decode(n, op.nx, op.ny);
+        const double rho = op.rec[n].x;
+        const double2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
+        const double2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
+        const long long sy = op.nx, sz = (long long)op.nx * op.ny;
+        double2 e[6];
+        for (int d = 0; d < 6; ++d) e[d] = make_double2(0.0, 0.0);
+        auto edge = [&](int dir, long long m, double2 F) { e[dir] = cscale(F, 2.0 / (rho + op.rec[m].x)); };
+        if (p.i > 0) edge(0, n - 1, cmul(fyz, op.Q[0][p.i - 1]));
+        if (p.i < op.nx - 1) edge(1, n + 1, cmul(fyz, op.Q[0][p.i]));
+        if (p.j > 0) edge(2, n - sy, cmul(fxz, op.Q[1][p.j - 1]));
+        if (p.j < op.ny - 1) edge(3, n + sy, cmul(fxz, op.Q[1][p.j]));
+        if (p.k > 0) edge(4, n - sz, cmul(fxy, op.Q[2][p.k - 1]));
+        if (p.k < op.nz - 1) edge(5, n + sz, cmul(fxy, op.Q[2][p.k]));
+        for (int d = 0; d < 6; ++d) e64[6 * n + d] = e[d];
+    }
+}
+
 // Complex64 row coefficients c_nd = R_n e_nd s_d (conj(e_nd) and the adjoint
 // scalings for K'), evaluated in FP64 by the same row code as the FP64
 // operator with a unit value in direction d only, then rounded once to fp32.
@@ -452,6 +477,8 @@ int usv_operator_build(const usv_scene* scene, const double* rho, const double* 
     a.rec32a = reinterpret_cast<float4*>(buf + L.rec32a);
     a.flag = reinterpret_cast<int*>(buf + L.flag);
     k_build<<<grid_for(a.op.n), 256, 0, strm>>>(a);
+    USV_CUDA_TRY(cudaGetLastError());
+    k_edges<<<grid_for(a.op.n), 256, 0, strm>>>(a.op, reinterpret_cast<double2*>(buf + L.e64));
     USV_CUDA_TRY(cudaGetLastError());
     k_coef<false><<<grid_for(a.op.n), 256, 0, strm>>>(
         make_view<double>(s, op_buf, false), reinterpret_cast<float4*>(buf + L.cf32f));

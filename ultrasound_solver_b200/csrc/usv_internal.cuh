@@ -142,7 +142,7 @@ __device__ __forceinline__ void bf_sq(float& rr, float& ii, unsigned y) {
 // so host and device agree without storing the layout itself.
 struct Layout {
     size_t tab64[3], q64[3], tab32[3], q32[3];
-    size_t rec64f, rec64a, d64, rec32f, rec32a, cf32f, cf32a, flag;
+    size_t rec64f, rec64a, d64, e64, rec32f, rec32a, cf32f, cf32a, flag;
     size_t total;
 };
 
@@ -162,6 +162,10 @@ inline Layout make_layout(const usv_scene& s) {
     L.rec64f = off; off = align_up(off + sizeof(double4) * n);
     L.rec64a = off; off = align_up(off + sizeof(double4) * n);
     L.d64 = off;    off = align_up(off + sizeof(double2) * n);
+    // FP64 edge coefficients e_nd = F_d 2/(rho_n + rho_d) of A, six per node
+    // (zero for a missing neighbour); A is symmetric off the diagonal, so the
+    // same array gives the A^H rows (conj(e))
+    L.e64 = off;    off = align_up(off + 6 * sizeof(double2) * n);
     L.rec32f = off; off = align_up(off + sizeof(float4) * n);
     L.rec32a = off; off = align_up(off + sizeof(float4) * n);
     // complex64 row coefficients c_nd = R_n e_nd s_d of the six neighbour
@@ -186,6 +190,7 @@ template <typename R> struct OpView {
     const C4* rec;          // {rho, R, s.re, s.im} (forward or adjoint)
     const double2* d;       // diagonal A_ii (fp64 path only)
     const float4* cf;       // complex64 path: row coefficients, 3 float4 per node
+    const double2* e64;     // FP64 edge coefficients of A, 6 per node
 };
 
 inline unsigned soft_mask(const usv_scene& s) {
@@ -212,6 +217,7 @@ inline OpView<R> make_view(const usv_scene& s, const void* buf, bool adjoint) {
     v.rec = reinterpret_cast<const typename OpView<R>::C4*>(b + rec);
     v.d = reinterpret_cast<const double2*>(b + L.d64);
     v.cf = dbl ? nullptr : reinterpret_cast<const float4*>(b + (adjoint ? L.cf32a : L.cf32f));
+    v.e64 = reinterpret_cast<const double2*>(b + L.e64);
     return v;
 }
 
@@ -490,38 +496,26 @@ __device__ __forceinline__ double2 a_row(const OpView<double>& op,
     const double2 xn = x[n];
     const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
     if (!H && fixed) return ABS ? make_double2(cabs(xn), 0.0) : xn;
-    const double rho = op.rec[n].x;
     const double2 d = op.d[n];
     double2 acc = ABS ? make_double2(cabs(d) * cabs(xn), 0.0) : (H ? cmulc(d, xn) : cmul(d, xn));
-    const double2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
-    const double2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
-    auto edge = [&](long long m, double2 F, bool nb_fixed) {
+    const double2* en = op.e64 + 6 * n;  // k_edges: F_d 2/(rho_n + rho_d)
+    auto edge = [&](int dir, long long m, bool nb_fixed) {
         if (H && nb_fixed) return;
-        const double g = 2.0 / (rho + op.rec[m].x);
-        const double2 e = cscale(F, g);
+        const double2 e = en[dir];
         const double2 xm = x[m];
         if (ABS) acc.x += cabs(e) * cabs(xm);
         else acc = cadd(acc, H ? cmulc(e, xm) : cmul(e, xm));
     };
     const long long sy = op.nx, sz = (long long)op.nx * op.ny;
-    if (p.i > 0)
-        edge(n - 1, cmul(fyz, op.Q[0][p.i - 1]),
-             H && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.i > 0) edge(0, n - 1, H && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
     if (p.i < op.nx - 1)
-        edge(n + 1, cmul(fyz, op.Q[0][p.i]),
-             H && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
-    if (p.j > 0)
-        edge(n - sy, cmul(fxz, op.Q[1][p.j - 1]),
-             H && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
+        edge(1, n + 1, H && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.j > 0) edge(2, n - sy, H && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
     if (p.j < op.ny - 1)
-        edge(n + sy, cmul(fxz, op.Q[1][p.j]),
-             H && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
-    if (p.k > 0)
-        edge(n - sz, cmul(fxy, op.Q[2][p.k - 1]),
-             H && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
+        edge(3, n + sy, H && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
+    if (p.k > 0) edge(4, n - sz, H && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
     if (p.k < op.nz - 1)
-        edge(n + sz, cmul(fxy, op.Q[2][p.k]),
-             H && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
+        edge(5, n + sz, H && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
     return acc;
 }
 
