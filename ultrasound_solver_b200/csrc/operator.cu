@@ -188,8 +188,9 @@ __global__ void __launch_bounds__(256) k_build(BuildArgs a) {
 
 // FP64 edge coefficients of A for the FP64 rows (usv_internal.cuh: a_row):
 // e_nd = F_d 2/(rho_n + rho_d), F_d the face product of the direction tables,
-// by the same expressions a row used to evaluate on the fly (bit-identical);
-// zero where the neighbour is missing.
+// by the same expressions a row used to evaluate on the fly (equal to the
+// last bits: the on-the-fly form may fuse the face product into the row's
+// FMAs); zero where the neighbour is missing.
 __global__ void __launch_bounds__(256) k_edges(OpView<double> op, double2* e64) {
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
          n += (long long)gridDim.x * blockDim.x) {
