@@ -1010,8 +1010,12 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
     extern __shared__ __align__(16) uint4 stg[];
     __shared__ double2 ys[USV_MAX_RESTART];
+    __shared__ float2 yf[USV_MAX_RESTART];
     const int L = g.len[b];
-    for (int t = threadIdx.x; t < L; t += kThreads) ys[t] = g.y[(long long)b * g.m + t];
+    for (int t = threadIdx.x; t < L; t += kThreads) {
+        ys[t] = g.y[(long long)b * g.m + t];
+        yf[t] = make_float2(float(ys[t].x), float(ys[t].y));
+    }
     const long long N = op.n;
     // solution vectors: U_t (t < kc) of the cycle's pair, then Krylov slots
     const CycleBasis<C2> cb = cycle_basis(const_cast<C2*>(V), g, b);
@@ -1022,10 +1026,32 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
         double2 acc[kPairs][2];
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) acc[k][0] = acc[k][1] = make_double2(0.0, 0.0);
-        stream_basis<C2>(stg, cb.U + n0, cb.V + n0, cb.kc, g.nv, L - 1, len, false,
-                         [&](int t, int k, int c, typename MathT<C2>::T2 vv) {
-            acc[k][c] = cadd(acc[k][c], cmul(ys[t], make_double2(vv.x, vv.y)));
-        });
+        if constexpr (std::is_same<C2, bf2>::value) {
+            // bfloat16: the correction W y in fp32 (packed fp32x2 FMAs, like
+            // k_orth; widening every basis value to FP64 would load the
+            // conversion unit), added to the FP64 solution below
+            float2 pa[kPairs][2], pb[kPairs][2];
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k)
+                pa[k][0] = pa[k][1] = pb[k][0] = pb[k][1] = make_float2(0.f, 0.f);
+            stream_basis<C2>(stg, cb.U + n0, cb.V + n0, cb.kc, g.nv, L - 1, len, false,
+                             [&](int t, int k, int c, float2 vv) {
+                const float2 y = yf[t];
+                pa[k][c] = ffma2(vv, make_float2(y.x, y.x), pa[k][c]);
+                pb[k][c] = ffma2(vv, make_float2(y.y, -y.y), pb[k][c]);  // (y.im v.re, -y.im v.im)
+            });
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    acc[k][c] = make_double2(double(pa[k][c].x) + double(pb[k][c].y),
+                                             double(pa[k][c].y) + double(pb[k][c].x));
+        } else {
+            stream_basis<C2>(stg, cb.U + n0, cb.V + n0, cb.kc, g.nv, L - 1, len, false,
+                             [&](int t, int k, int c, typename MathT<C2>::T2 vv) {
+                acc[k][c] = cadd(acc[k][c], cmul(ys[t], make_double2(vv.x, vv.y)));
+            });
+        }
         double2* xb = x + b * ld + n0;
 #pragma unroll
         for (int k = 0; k < kPairs; ++k)
