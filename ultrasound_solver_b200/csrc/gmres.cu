@@ -1,18 +1,19 @@
 // Restarted, right-preconditioned GMRES(m) on the row-scaled Jacobi operator
 // K = R A S (or K' = R' A^H S' for the adjoint), batched over right-hand
-// sides, with Krylov vectors in complex64 (USV_PREC_MIXED) or complex128
-// (USV_PREC_FP64).
+// sides, with Krylov vectors in complex64 (USV_PREC_MIXED), bfloat16
+// (USV_PREC_MIXED_BF16) or complex128 (USV_PREC_FP64).
 //
 // Algorithm parity: iterative_solver.py:30-104 drives CuPy's gmres
 // (cupyx.scipy.sparse.linalg.gmres, cupy>=14, not vendored by the
 // reference): x0 = 0, residual r = Rb - K x tested against rtol*||Rb|| only
 // at restarts, one-pass classical Gram-Schmidt, all m steps per cycle,
 // least squares of the (m+1) x m Hessenberg, x += V y, solution S x.
-// Here the restart residual r = R (b - A x_sol) and the solution update
-// x_sol += S V y are always FP64; the Gram-Schmidt dots and the Hessenberg /
-// Givens least squares are FP64 on the device; only the Krylov vectors and
-// the in-cycle stencil use the vector precision. With complex64 vectors this
-// is GMRES with FP64 iterative refinement at every restart.
+// Here the restart residual r = R (b - A x_sol) and the solution x_sol are
+// always FP64 (the correction V y is summed in FP64, in fp32 for bfloat16
+// vectors); the Gram-Schmidt reductions and the Hessenberg / Givens least
+// squares are FP64 on the device; the Krylov vectors and the in-cycle stencil
+// use the vector precision. With complex64 or bfloat16 vectors this is GMRES
+// with FP64 iterative refinement at every restart.
 //
 // Per Arnoldi step two kernels run over (node chunk, RHS):
 //   k_dots : w = sigma_j K u_j (stencil) stored as u_{j+1}; partial dots
@@ -1000,7 +1001,7 @@ __global__ void __launch_bounds__(128) k_lsq(GState g) {
     }
 }
 
-// ------------------------------------------------------------ solution update (fp64)
+// ------------------------------------------------------------ solution update
 template <typename S>
 __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S* V, double2* x,
                                                      long long ld, GState g) {
