@@ -170,7 +170,8 @@ int usv_operator_bytes(const usv_scene* scene, size_t* bytes);
 int usv_operator_build(const usv_scene* scene, const double* rho, const double* c,
                        void* op_buf, size_t op_bytes, void* stream);
 /* y[:, b] = OP x[:, b] for b < nrhs; `precision` selects complex128/64 for
- * USV_APPLY_K/KH (the fp64-only variants ignore it). */
+ * USV_APPLY_K/KH (the fp64-only variants ignore it). x and y must not
+ * overlap (a row reads x at its six neighbours). */
 int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant,
                        int precision, const void* x, void* y, int nrhs, int64_t ld,
                        void* stream);
