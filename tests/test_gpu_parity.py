@@ -156,6 +156,21 @@ def test_recycled_gmres_matches_direct(golden, precision):
         assert rel(x[k], golden["G"][:, k]) <= 1e-6
 
 
+@pytest.mark.parametrize("k", [1, 3, 5, 13])
+def test_recycled_bf16_other_sizes(k):
+    """bfloat16 GCRO-DR(30, k) with recycled-space sizes whose tensor-core tiles
+    are partly empty (k = 1, 3, 5, 13) reaches the direct solution for a batch
+    of columns."""
+    from tests.conftest import load_golden
+    g = load_golden("mixed")
+    s = golden_solver(g, precision="bf16", gmres_rtol=1e-10, gmres_maxiter=20000,
+                      gmres_recycle=k, gmres_recycle_every=1)
+    cols = s.sources.column_rhs(s.transducers.amplitudes)[:3]
+    x = s.solve_rhs_device(cols).cpu().numpy()
+    for c in range(x.shape[0]):
+        assert rel(x[c], g["G"][:, c]) <= 1e-6
+
+
 def test_recycling_reduces_iterations(golden):
     """On a scene where restarted GMRES(30) needs many cycles, deflated restarting with
     8 recycled vectors needs fewer inner iterations to the same residual."""
