@@ -522,11 +522,6 @@ __device__ __forceinline__ void stream_basis(uint4* stg, const C2* base0, const 
 // all warps work.
 constexpr int kDotUnroll = 8;
 constexpr int kDotsThreads = 512;
-// Arnoldi stencil: z-marching kernel ahead of the dots (true) or fused into
-// k_dots (false). The z-marching split measured 6-10% slower per iteration at
-// 128^3 (complex64 and bfloat16): the fused form keeps w in shared memory and
-// saves a launch per step.
-constexpr bool kZMarchStencil = false;
 
 template <typename Y, typename C2> __device__ __forceinline__ Y as_ys(C2 v) { return v; }
 template <> __device__ __forceinline__ double2 as_ys<double2, float2>(float2 v) {
@@ -561,36 +556,16 @@ template <> struct LaneLoad<double2> {
     __device__ __forceinline__ double2 get(int i) const { return i ? b : a; }
 };
 
-// Arnoldi step j, stencil part in z-marching form (usv_internal.cuh:
-// zmarch_rows): w = sigma_j K u_j into slot j+1; k_dots (mode 2) then forms
-// the dots.
-template <typename R, typename S, bool ADJ>
-__global__ void __launch_bounds__(kZTX * kZTY) k_stencil25(OpView<R> op, S* V, GState g, int j,
-                                                           int zseg) {
-    const int b = blockIdx.z;
-    if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
-    const CycleBasis<S> cb = cycle_basis(V, g, b);
-    if (j < cb.kc) return;
-    __shared__ ZTile<R> sm;
-    const S* uj = cb.V + (long long)j * g.nv;
-    S* w = cb.V + (long long)(j + 1) * g.nv;
-    const R sj = R(g.sigma[b * (g.m + 1) + j]);
-    const int z0 = blockIdx.y * zseg, z1 = min(op.nz, z0 + zseg);
-    zmarch_rows<R, ADJ>(op, uj, blockIdx.x, z0, z1, sm, [&](long long n, typename Tr<R>::c2 v) {
-        w[n] = narrow<S>(cscale(v, sj));
-    });
-}
-
 // Arnoldi step j, part 1: each CTA computes its chunk of w = sigma_j K u_j
 // (stencil) into shared and global memory, then the dots <sigma_t u_t, w>,
 // t <= j, and ||w||^2. (A separate stencil kernel ahead of a streaming dots
-// kernel measured 9% slower per iteration at 128^3: the extra launch and the
-// re-read of w cost more than the overlap of the two phases gains. Streaming
-// the dots per thread through the cp.async pipeline instead of warp tasks
-// measured the same for bfloat16 and 8% slower for complex64.)
+// kernel, plain or z-marching, measured 6-10% slower per iteration at 128^3:
+// the extra launch and the re-read of w cost more than the overlap of the two
+// phases gains. Streaming the dots per thread through the cp.async pipeline
+// instead of warp tasks measured the same for bfloat16 and 8% slower for
+// complex64.)
 // mode 1 (recycled cycles): no stencil; the dots alpha_t = <C_t, r> of the
 // cycle's first residual r (slot kc) with the recycled C_t, t < kc.
-// mode 2: the Arnoldi dots of w = sigma_j K u_j already written by k_stencil25.
 template <typename R, typename S, bool ADJ, int NT>
 __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, int j, Step step,
                                                 int mode) {
@@ -1726,19 +1701,8 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     if (int e = grid_for((const void*)k_residual<ADJ, C2>, 256, 0, grid_res)) return e;
     if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0, grid_dots))
         return e;
-    int z_per_sm = 0;
-    USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &z_per_sm, (const void*)k_stencil25<R, S, ADJ>, kZTX * kZTY, 0));
-    const ZGrid zg = zmarch_grid(s.nx, s.ny, s.nz,
-                                 (z_per_sm > 0 ? z_per_sm : 1) * (sms > 0 ? sms : 148) / B);
-    const dim3 grid_z(zg.tiles, zg.runs, B);
     auto launch_dots = [&](cudaStream_t st, int j, int proj) {
-        if (proj || !kZMarchStencil) {
-            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
-        } else {
-            k_stencil25<R, S, ADJ><<<grid_z, kZTX * kZTY, 0, st>>>(opk, V, g, j, zg.zseg);
-            k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, 2);
-        }
+        k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
     };
     if (int e = grid_for((const void*)k_orth<S>, kThreads, pipe_smem, grid_orth)) return e;
     if (int e = grid_for((const void*)k_update<S>, kThreads, pipe_smem, grid_upd)) return e;

@@ -262,20 +262,6 @@ __global__ void __launch_bounds__(256) k_apply_fp64(OpView<double> op, const dou
     }
 }
 
-template <typename R, bool ADJ>
-__global__ void __launch_bounds__(256) k_apply_k(OpView<R> op, const typename Tr<R>::c2* x,
-                                                 typename Tr<R>::c2* y, long long ld, Step step) {
-    const int b = blockIdx.y;
-    const auto* xb = x + b * ld;
-    auto* yb = y + b * ld;
-    long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    Node p = decode(n, op.nx, op.ny);
-    for (; n < op.n; n += (long long)gridDim.x * blockDim.x) {
-        yb[n] = k_row<R, ADJ>(op, xb, n, p);
-        advance(p, step, op.nx, op.ny);
-    }
-}
-
 // y = K x for complex64 from the precomputed row coefficients: one thread per
 // node reads the node's coefficients once and applies them to every
 // right-hand side (nrhs vectors at stride ld), so a batch reads the operator
@@ -358,10 +344,11 @@ __global__ void __launch_bounds__(256) k_apply_kc_rhs(OpView<float> op, const fl
     }
 }
 
-// y = K x through the z-marching tile kernel (usv_internal.cuh: zmarch_rows).
-// usv_operator_apply K / K^H: z-marching kernel for complex128 (74 vs 97 us at
-// 128^3); complex64 uses the coefficient rows (k_apply_kc_rhs / k_apply_kc).
-constexpr bool kZMarch64 = true, kZMarch32 = false;
+// y = K x through the z-marching tile kernel (usv_internal.cuh: zmarch_rows):
+// usv_operator_apply K / K^H in complex128 (74 us at 128^3 against 97 us for a
+// row-per-thread kernel); complex64 uses the coefficient rows (k_apply_kc_rhs /
+// k_apply_kc; its z-marching form measured 40 us against 35 us for the
+// row-per-thread kernel of that time).
 template <typename R, bool ADJ>
 __global__ void __launch_bounds__(kZTX * kZTY) k_apply_k25(OpView<R> op, const typename Tr<R>::c2* x,
                                                            typename Tr<R>::c2* y, long long ld,
@@ -523,36 +510,22 @@ int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant, 
         case USV_APPLY_K:
         case USV_APPLY_KH: {
             const bool adj = variant == USV_APPLY_KH;
-            // z-marching grid: tiles x runs of planes x right-hand sides
-            int dev = 0, sms = 148, per_sm = 1;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (precision == USV_PREC_FP64)
+            if (precision == USV_PREC_FP64) {
+                // z-marching grid: tiles x runs of planes x right-hand sides
+                int dev = 0, sms = 148, per_sm = 1;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                     &per_sm, adj ? (const void*)k_apply_k25<double, true> : (const void*)k_apply_k25<double, false>,
                     kZTX * kZTY, 0);
-            else
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                    &per_sm, adj ? (const void*)k_apply_k25<float, true> : (const void*)k_apply_k25<float, false>,
-                    kZTX * kZTY, 0);
-            const ZGrid zg = zmarch_grid(s.nx, s.ny, s.nz, (per_sm > 0 ? per_sm : 1) * sms / nrhs);
-            const int zseg = zg.zseg;
-            const dim3 g25(zg.tiles, zg.runs, nrhs);
-            if (precision == USV_PREC_FP64) {
+                const ZGrid zg = zmarch_grid(s.nx, s.ny, s.nz, (per_sm > 0 ? per_sm : 1) * sms / nrhs);
+                const dim3 g25(zg.tiles, zg.runs, nrhs);
                 auto v = make_view<double>(s, op_buf, adj);
-                if (kZMarch64) {
-                    if (adj) k_apply_k25<double, true><<<g25, kZTX * kZTY, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, zseg);
-                    else k_apply_k25<double, false><<<g25, kZTX * kZTY, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, zseg);
-                } else {
-                    if (adj) k_apply_k<double, true><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, step);
-                    else k_apply_k<double, false><<<grid, 256, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, step);
-                }
+                if (adj) k_apply_k25<double, true><<<g25, kZTX * kZTY, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, zg.zseg);
+                else k_apply_k25<double, false><<<g25, kZTX * kZTY, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, zg.zseg);
             } else if (precision == USV_PREC_MIXED) {
                 auto v = make_view<float>(s, op_buf, adj);
-                if (kZMarch32) {
-                    if (adj) k_apply_k25<float, true><<<g25, kZTX * kZTY, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, zseg);
-                    else k_apply_k25<float, false><<<g25, kZTX * kZTY, 0, strm>>>(v, (const float2*)x, (float2*)y, ld, zseg);
-                } else if (nrhs <= 8 && s.nz <= 65535) {
+                if (nrhs <= 8 && s.nz <= 65535) {
                     const float2* xf = (const float2*)x;
                     float2* yf = (float2*)y;
                     const int r = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : 8;
