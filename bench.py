@@ -175,9 +175,21 @@ def max_over_ranks(value, world):
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(world, steps, batch, ms_max):
+    """Whole-job RHS solves/s: every rank solves `steps` batches of `batch`
+    independent right-hand sides (replicas), timed by the slowest rank."""
+    return world * steps * batch / (ms_max / 1000.0)
+
+
+def replica_seed(rank):
+    """Seed of a rank's phase vectors: distinct right-hand sides per replica."""
+    return 1 + rank
 
 
 # ---------------------------------------------------------------- workload
@@ -211,7 +223,7 @@ def run_ours(args):
     rank, world, local = dist_setup(args.gpus)
     cfg, desc = workload_config(args)
     solver = W.build_solver(cfg, seed=0)
-    rng = np.random.default_rng(1 + rank)
+    rng = np.random.default_rng(replica_seed(rank))
     solver.assemble_matrix()
     rhs_list = []
     for _ in range(args.batch):
@@ -265,7 +277,7 @@ def run_ours(args):
     barrier(world)
     ms_local = start.elapsed_time(stop)
     ms = max_over_ranks(ms_local, world)
-    value = world * args.steps * args.batch / (ms / 1000.0)
+    value = job_throughput(world, args.steps, args.batch, ms)
     stats = dict(it.last_stats[0])
 
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
