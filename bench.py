@@ -354,6 +354,10 @@ def run_ours(args):
             "achieved": bytes_k / (ms_k / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
             "frac": bytes_k / (ms_k / 1e3) / 1e9 / peak, "us_per_launch": 1000.0 * ms_k,
             "bytes_per_launch": bytes_k, "l2": "inputs larger than L2 (20 launches back to back)",
+            # compulsory traffic of a minimal representation (3 real face
+            # coefficients + k^2 per node, fp32) against the same time
+            "compulsory_bytes_per_launch": nn * (16.0 + args.batch * 16.0),
+            "compulsory_frac": nn * (16.0 + args.batch * 16.0) / (ms_k / 1e3) / 1e9 / peak,
             "fp64_A": {"kernel": f"k_apply_fp64 (complex128 A rows), {args.batch} RHS per launch",
                        "achieved": bytes_a / (ms_a / 1e3) / 1e9,
                        "frac": bytes_a / (ms_a / 1e3) / 1e9 / peak,
