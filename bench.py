@@ -350,7 +350,7 @@ def run_ours(args):
         bytes_a = nn * (112.0 + args.batch * 32.0)
         peak, peak_kind = measured_peak()
         out["stencil"] = {
-            "kernel": f"k_apply_kc (complex64 K rows), {args.batch} RHS per launch",
+            "kernel": f"k_apply_kc_rhs (complex64 K rows), {args.batch} RHS per launch",
             "achieved": bytes_k / (ms_k / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
             "frac": bytes_k / (ms_k / 1e3) / 1e9 / peak, "us_per_launch": 1000.0 * ms_k,
             "bytes_per_launch": bytes_k, "l2": "inputs larger than L2 (20 launches back to back)",
