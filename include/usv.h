@@ -48,7 +48,7 @@
 extern "C" {
 #endif
 
-#define USV_ABI_VERSION 2
+#define USV_ABI_VERSION 3
 
 /* status codes */
 #define USV_OK 0
@@ -61,6 +61,7 @@ extern "C" {
 #define USV_ERR_SOURCE_SOFT 7    /* deposited aperture touches a soft face       */
 #define USV_ERR_SOURCE_CLEARANCE 8 /* aperture closer than one cell to a side    */
 #define USV_ERR_TOO_LARGE 9      /* size beyond a fixed internal maximum          */
+#define USV_ERR_DEVICE_TIMEOUT 10 /* a bounded device-side wait ran out          */
 
 /* face kinds, faces in the reference order -x,+x,-y,+y,-z,+z */
 #define USV_FACE_REFLECTING 0
@@ -131,6 +132,10 @@ typedef struct usv_gmres_params {
                                     cycle (k <= min(16, m-1)); 0: plain GMRES(m) */
     int32_t recycle_every;       /* recompute the recycled space after every n-th
                                     cycle (0 or 1: every cycle)                  */
+    int32_t max_ctas;            /* cap on the CTAs per right-hand side of the
+                                    streaming kernels (each CTA then loops over
+                                    more node chunks); 0 = fill the GPU          */
+    int32_t reserved;
 } usv_gmres_params;
 
 typedef struct usv_gmres_stats {
@@ -239,12 +244,20 @@ int usv_basis_adjoint(const void* basis, int64_t n, int m, int basis_precision,
  * file-scope device array that every GPU loading this library holds until
  * exit; m (emitters) is limited to 4096, larger m returns USV_ERR_TOO_LARGE.
  * The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress) and caches it for the life of the process; make
+ * that first call before any stream capture, and do not use this entry point
+ * on a device after cudaDeviceReset (the cached address is then stale).
  * All calls share the array: calls that overlap on the GPU (other streams or
  * threads) race and must be serialised by the caller. */
 int usv_basis_adjoint_noalloc(const void* basis, int64_t n, int m, int basis_precision,
                               const void* cotangent, const double* phases,
                               double* response, double* grad, void* stream);
+/* out (device complex128, p x m, row-major) = trilinear interpolation of the
+ * basis columns at p points (device fp64, p x 3, metres from node (0,0,0)).
+ * Points are expected inside [0, (n-1) dx] per axis (the Python host checks
+ * this, as the reference does); a point outside extrapolates linearly from
+ * the nearest edge cell and a non-finite point gives NaN, never a load
+ * outside the basis. */
 int usv_basis_target_response(const void* basis, int64_t nx, int64_t ny, int64_t nz,
                               int m, int basis_precision, const double* points, int p,
                               double dx, void* out, void* stream);

@@ -18,6 +18,8 @@ it follows (paths relative to the reference project root):
 * material VJP                        src/algorithm/physics/conservative_helmholtz.py:151-175
 * phase basis field / VJP / trilinear src/algorithm/training/phase_response_basis.py:139-253
 * focal losses and background mask   src/algorithm/training/phase_adjoint_optimizer.py:142-414
+* Adam on the phases (adjoint         src/algorithm/baselines/adjoint/__init__.py:38-83
+  baseline, optimizer "adam")
 
 The GMRES arithmetic of the reference lives in a third-party dependency that
 the reference does not vendor: ``cupy-cuda12x[ctk]>=14.0.0``
@@ -615,3 +617,45 @@ def build_scene(cfg, material_fields=None, phases=None):
     sc.phases = np.zeros(len(centers)) if phases is None else np.asarray(phases, float)
     sc.rhs = B @ (sc.amplitudes * np.exp(1j * sc.phases))
     return sc
+
+
+# --------------------------------------------------------------------------
+# Adam phase optimisation (src/algorithm/baselines/adjoint/__init__.py:38-83)
+# --------------------------------------------------------------------------
+def phase_gradient(B, amplitudes, lam, phases):
+    """dL/dphi_m = Re(conj((B^H lam)_m) a_m i e^{i phi_m}) for dL = Re(g^H du),
+    lam = A^-H g (the basis VJP of phase_response_basis.py:208-253 with
+    G = A^-1 B diag(a))."""
+    proj = B.conj().T @ lam
+    return np.real(np.conj(proj) * np.asarray(amplitudes) * 1j * np.exp(1j * np.asarray(phases)))
+
+
+def adam_trajectory(A, B, amplitudes, phases0, loss_fn, steps, learning_rate=0.05):
+    """Phases and losses of `steps` Adam updates (adjoint/__init__.py:71-83),
+    every evaluation a direct forward solve and a direct A^H solve.
+    loss_fn(u) -> (loss, cotangent). Returns (phases per evaluation,
+    losses per evaluation, gradients per evaluation)."""
+    lu = spla.splu(sp.csc_matrix(A))
+    amps = np.asarray(amplitudes, dtype=np.float64)
+
+    def evaluate(ph):
+        u = lu.solve(B @ (amps * np.exp(1j * ph)))
+        loss, cot = loss_fn(u)
+        lam = lu.solve(np.asarray(cot, dtype=np.complex128).ravel(), trans="H")
+        return loss, phase_gradient(B, amps, lam, ph)
+
+    ph = np.asarray(phases0, dtype=np.float64).copy()
+    loss, grad = evaluate(ph)
+    phases, losses, grads = [ph.copy()], [loss], [grad]
+    first = np.zeros_like(ph)
+    second = np.zeros_like(ph)
+    for step in range(1, steps + 1):
+        first = 0.9 * first + 0.1 * grad
+        second = 0.999 * second + 0.001 * grad ** 2
+        ph = ph - learning_rate * (first / (1 - 0.9 ** step)) / (
+            np.sqrt(second / (1 - 0.999 ** step)) + 1e-8)
+        loss, grad = evaluate(ph)
+        phases.append(ph.copy())
+        losses.append(loss)
+        grads.append(grad)
+    return phases, losses, grads

@@ -188,6 +188,106 @@ def make_scene(name, cfg, reference_src):
     print(name, shape, "nnz", A.nnz, "m", m)
 
 
+# Mid-size scene: large enough that the streaming GMRES kernels work through
+# many node chunks (with a capped CTA count every CTA loops over several), with
+# a seeded random medium, a blended high-contrast sphere and all face kinds.
+MID = {
+    "mode": "phase_optimization",
+    "physics": {"sound_speed": 343.0, "medium_density": 1.2},
+    "transducer_specs": {"frequency": 40000.0, "array_n": 2, "diameter": 0.006,
+                         "pitch": 0.008, "geometry": "ideal_grid",
+                         "source_radial_order": 16, "source_angular_order": 32},
+    "domain": {"box_size": [0.035, 0.031, 0.029], "grid_size": [36, 32, 30]},
+    "boundary_conditions": {"-x": "open",
+                            "+x": {"type": "impedance", "impedance": [826.0, -40.0]},
+                            "-y": "soft", "+y": "open", "-z": "reflecting", "+z": "open"},
+    "targets": [{"point": [0.0175, 0.0155, 0.018]}],
+    "obstacles": [],
+    "solver": {"pml": {"cells": 6, "strength": 2.0, "order": 2, "faces": ["+y", "+z"]}},
+    "training": {"background_weight": 0.05, "target_radius": 0.002,
+                 "source_exclusion_layers": 2, "sidelobe_temperature": 25.0},
+}
+MID_ADJOINT_RHS = 3
+
+
+def mid_materials(shape, dx):
+    """Seeded random medium (Gaussian field smoothed over 2 cells, unit std,
+    clipped to +-3; c = 343 (1 + 0.05 g), rho = 1.2 (1 + 0.1 g')) with a
+    rho = 1250 / c = 2200 sphere (radius 5 mm) blended by the reference's
+    smoothed step over 1.2 cells."""
+    from scipy.ndimage import gaussian_filter
+    from algorithm.physics.warp_utils import blend_obstacle_material
+    rng = np.random.default_rng(40)
+    fields = []
+    for _ in range(2):
+        g = gaussian_filter(rng.standard_normal(shape), 2.0)
+        fields.append(np.clip(g / g.std(), -3.0, 3.0))
+    c = 343.0 * (1 + 0.05 * fields[0])
+    rho = 1.2 * (1 + 0.1 * fields[1])
+    coords = np.ogrid[:shape[0], :shape[1], :shape[2]]
+    centre = (0.018, 0.016, 0.015)
+    sdf = np.sqrt(sum((coords[a] * dx - centre[a]) ** 2 for a in range(3))) - 0.005
+    t = np.clip(sdf / (1.2 * dx), -1, 1)
+    h = .5 * (1 + t + np.sin(np.pi * t) / np.pi)
+    return blend_obstacle_material(h, 1250.0, 2200.0, rho, c)
+
+
+def make_mid(reference_src):
+    """golden_mid.npz: the reference's direct solutions of a 36 x 32 x 30 scene.
+
+    Stored: the material fields, the source columns (z = 0 plane), the
+    single-emitter responses G[:, k] = A^-1 (a_k B[:, k]) and three adjoint
+    solutions A^-H g (solutions rounded once to complex64: 6e-8 relative, far
+    below the 1e-6 parity bar), and A x for a deterministic probe vector (pins
+    the assembly without storing the matrix)."""
+    from algorithm.config import SimulationConfig
+    from algorithm.solvers.helmholtz_solver import HelmholtzDirectSolver
+
+    cfg = MID
+    with tempfile.TemporaryDirectory() as tmp:
+        path = Path(tmp) / "mid.yaml"
+        path.write_text(yaml.safe_dump(_yaml_config(cfg)))
+        config = SimulationConfig.from_yaml(str(path))
+        solver = HelmholtzDirectSolver(config)
+        shape = tuple(config.domain.grid_size)
+        n = int(np.prod(shape))
+        rho, c = mid_materials(shape, config.domain.dx)
+        solver.set_material_fields(rho, c)
+        m = solver.transducers.num_transducers
+        rng = np.random.default_rng(41)
+        phases = rng.uniform(0, 2 * np.pi, m)
+        solver.set_phases(phases)
+        solver.assemble_matrix()
+        rhs = solver.update_rhs()
+        A = solver.A_cached_csr_cpu.tocsr()
+        B = solver.warp_engine.source_columns.tocsr()
+        nxy = shape[0] * shape[1]
+        assert B[nxy:].nnz == 0
+        lu = spla.splu(sp.csc_matrix(A))
+        amps = solver.transducers.amplitudes
+        G = np.column_stack([lu.solve(B[:, k].toarray().ravel() * amps[k]) for k in range(m)])
+        x = lu.solve(rhs)
+        # superposition of the single-emitter solves (LU rounding ~1e-9 here)
+        assert np.linalg.norm(G @ np.exp(1j * phases) - x) <= 1e-7 * np.linalg.norm(x)
+        g = (rng.standard_normal((n, MID_ADJOINT_RHS))
+             + 1j * rng.standard_normal((n, MID_ADJOINT_RHS))).astype(np.complex64)
+        lam = lu.solve(g.astype(np.complex128), trans="H")
+        probe = mid_probe(n)
+        out = dict(cfg_json=json.dumps(cfg, sort_keys=True), shape=np.array(shape),
+                   dx=config.domain.dx, omega=config.omega, material_rho=rho, material_c=c,
+                   phases=phases, B_top=B[:nxy].toarray(), rhs=rhs,
+                   G=G.astype(np.complex64), adj_rhs=g, adj_sol=lam.astype(np.complex64),
+                   Ax_probe=A @ probe, fixed=solver.warp_engine.fixed_dofs())
+    np.savez_compressed(HERE / "golden_mid.npz", **out)
+    print("mid", shape, "nnz", A.nnz, "m", m)
+
+
+def mid_probe(n):
+    """Deterministic complex probe vector for the assembly check."""
+    t = np.arange(n, dtype=np.float64)
+    return np.cos(0.37 * t) + 1j * np.sin(0.11 * t + 0.5)
+
+
 def make_blend(reference_src):
     from algorithm.physics.warp_utils import blend_obstacle_material
     h = np.linspace(0.0, 1.0, 11)
@@ -196,12 +296,22 @@ def make_blend(reference_src):
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference").resolve()
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [scene ...]   "
+                 "(the checkout that holds src/algorithm)")
+    ref = Path(sys.argv[1]).resolve()
+    if not (ref / "src" / "algorithm").is_dir():
+        sys.exit(f"{ref} does not hold src/algorithm")
+    only = set(sys.argv[2:])
     sys.path.insert(0, str(ref / "src"))
     _install_stubs()
-    make_blend(ref)
+    if not only or "blend" in only:
+        make_blend(ref)
     for name, cfg in SCENES.items():
-        make_scene(name, cfg, ref)
+        if not only or name in only:
+            make_scene(name, cfg, ref)
+    if not only or "mid" in only:
+        make_mid(ref)
 
 
 if __name__ == "__main__":

@@ -56,4 +56,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden_surface.py REFERENCE_ROOT   (the checkout that holds src/algorithm)")
+    main(sys.argv[1])

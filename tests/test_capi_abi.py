@@ -29,13 +29,13 @@ def test_struct_sizes_match_header(lib):
     # natural C alignment of the structs in include/usv.h (4 bytes of padding before dx)
     assert ctypes.sizeof(_native.Scene) == 176
     assert _native.Scene.dx.offset == 40
-    assert ctypes.sizeof(_native.GmresParams) == 72
+    assert ctypes.sizeof(_native.GmresParams) == 80
     assert ctypes.sizeof(_native.GmresProfile) == 160
     assert ctypes.sizeof(_native.GmresStats) == 40
 
 
 def test_host_only_entry_points(lib):
-    assert lib.usv_abi_version() == 2
+    assert lib.usv_abi_version() == _native.ABI_VERSION == 3
     assert lib.usv_status_string(0) == b"ok"
     s = _native.Scene()
     s.nx = s.ny = s.nz = 9

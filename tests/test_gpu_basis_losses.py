@@ -154,3 +154,43 @@ def _rhs(golden, phases):
     nxy = golden["B_top"].shape[0]
     b[:nxy] = golden["B_top"] @ np.exp(1j * phases)
     return b
+
+
+def test_target_response_points_outside_the_grid():
+    """usv_basis_target_response through the C ABI with a point just below the
+    origin (extrapolated from the edge cell, all loads inside the basis), a
+    non-finite point (NaN response) and an interior point (the reference's
+    trilinear rows)."""
+    from ultrasound_solver_b200 import _native as N
+    nx, ny, nz, m, dx = 6, 5, 4, 3, 1e-3
+    n = nx * ny * nz
+    rng = np.random.default_rng(5)
+    G = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    pts = np.array([[-0.3e-3, 1.5e-3, 2.25e-3],
+                    [np.nan, 1e-3, 1e-3],
+                    [2.6e-3, 3.1e-3, 0.4e-3]])
+    dev = torch.device("cuda", 0)
+    Gd = torch.from_numpy(G).to(dev)
+    pd = torch.from_numpy(pts).to(dev)
+    out = torch.empty((3, m), dtype=torch.complex128, device=dev)
+    st = N.load().usv_basis_target_response(N.ptr(Gd), nx, ny, nz, m, N.PREC_FP64, N.ptr(pd), 3,
+                                            dx, N.ptr(out), N.stream_handle(torch, dev))
+    assert st == N.USV_OK
+    got = out.cpu().numpy()
+    # interior point: the reference's trilinear rows (oracle restatement)
+    want = O.basis_target_response(G.T, pts[2:], (nx, ny, nz), dx)[0]
+    assert rel(got[2], want) <= 1e-13
+    assert np.isnan(got[1]).all()
+    # below the origin in x: low corner 0, fraction -0.3 (linear extrapolation)
+    pos = pts[0] / dx
+    lo = np.array([0, 1, 2])
+    fr = pos - lo
+    acc = np.zeros(m, complex)
+    for ci in (0, 1):
+        for cj in (0, 1):
+            for ck in (0, 1):
+                w = ((fr[0] if ci else 1 - fr[0]) * (fr[1] if cj else 1 - fr[1])
+                     * (fr[2] if ck else 1 - fr[2]))
+                row = (lo[0] + ci) + nx * ((lo[1] + cj) + ny * (lo[2] + ck))
+                acc += w * G[:, row]
+    assert rel(got[0], acc) <= 1e-13

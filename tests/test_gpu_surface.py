@@ -44,3 +44,40 @@ def test_surface_solver_checks():
     from ultrasound_solver_b200.homogeneous_surface import HomogeneousSurfaceSolver
     with pytest.raises(ValueError, match="open/reflecting/impedance"):
         HomogeneousSurfaceSolver((8, 8, 8), 1e-3, 4e4, 343.0, 1.2, {"+z": "soft"})
+
+
+def test_solver_target_response_cache(tmp_path, monkeypatch):
+    """HelmholtzB200Solver.target_response with solver.target_response_cache:
+    the second call reads every response back from the store (no solve), a
+    new point is computed and added, and a different scene ignores the file."""
+    from ultrasound_solver_b200 import workloads as W
+    from ultrasound_solver_b200.config import SimulationConfig
+    from ultrasound_solver_b200.helmholtz_solver import HelmholtzB200Solver
+    from ultrasound_solver_b200.homogeneous_surface import HomogeneousSurfaceSolver
+
+    def make(freq):
+        d = W.scene_dict(24, 1e-3, 2, 6e-3, 4e-3, radial=8, angular=16)
+        d["transducer_specs"]["frequency"] = freq
+        d["solver"]["pml"] = {"cells": 4, "strength": 2.0, "order": 2}
+        d["solver"]["target_response_cache"] = str(tmp_path / "resp.npz")
+        return HelmholtzB200Solver(SimulationConfig.from_dict(d))
+
+    pts = np.array([[0.0115, 0.0115, 0.010], [0.010, 0.012, 0.013]])
+    s = make(40000.0)
+    first = s.target_response(pts)
+    assert (tmp_path / "resp.npz").exists()
+    calls = []
+    orig = HomogeneousSurfaceSolver.flux_target_response
+
+    def counting(self, masses, points):
+        calls.append(len(points))
+        return orig(self, masses, points)
+
+    monkeypatch.setattr(HomogeneousSurfaceSolver, "flux_target_response", counting)
+    again = make(40000.0).target_response(pts)
+    assert calls == [] and np.array_equal(again, first)
+    more = np.vstack((pts, [[0.012, 0.011, 0.008]]))
+    out = make(40000.0).target_response(more)
+    assert calls == [1] and np.array_equal(out[:2], first)
+    other = make(41000.0).target_response(pts)  # another scene: recomputed
+    assert calls == [1, 2] and not np.allclose(other, first)

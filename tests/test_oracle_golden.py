@@ -116,3 +116,32 @@ def test_gmres_restatement_converges_to_direct(golden):
     assert err < 1e-6
     assert res.scaled_residual <= 1e-10
     assert res.backward_error < 1e-8
+
+
+def test_mid_scene_assembly_and_solutions():
+    """Mid-size golden (36 x 32 x 30, random medium, blended sphere, every face
+    kind): the oracle's assembly against the reference's A x for a probe, its
+    sources, and the reference's direct solutions as residuals of its matrix."""
+    g = load_golden("mid")
+    _, sc = _scene(g)
+    n = int(np.prod(g["shape"]))
+    t = np.arange(n, dtype=np.float64)
+    probe = np.cos(0.37 * t) + 1j * np.sin(0.11 * t + 0.5)
+    ax = sc.A @ probe
+    assert np.linalg.norm(ax - g["Ax_probe"]) <= 1e-13 * np.linalg.norm(g["Ax_probe"])
+    nxy = int(g["shape"][0] * g["shape"][1])
+    np.testing.assert_allclose(sc.B[:nxy].toarray(), g["B_top"], rtol=1e-13,
+                               atol=1e-13 * np.abs(g["B_top"]).max())
+    assert np.linalg.norm(sc.rhs - g["rhs"]) <= 1e-13 * np.linalg.norm(g["rhs"])
+    np.testing.assert_array_equal(np.flatnonzero(sc.op.fixed.ravel(order="F")), g["fixed"])
+    # the stored solutions solve the oracle's system up to their complex64
+    # rounding (6e-8 per value; ||A|| ||x|| / ||b|| ~ 20 turns it into ~1e-6 of
+    # residual; a wrong assembly leaves O(1))
+    def resid(M, x, b):
+        return np.linalg.norm(M @ x - b) / np.linalg.norm(b)
+    for k in range(g["G"].shape[1]):
+        assert resid(sc.A, g["G"][:, k].astype(np.complex128), sc.B[:, k].toarray().ravel()) < 1e-5
+    AH = sc.A.conj().T.tocsr()
+    for k in range(g["adj_sol"].shape[1]):
+        assert resid(AH, g["adj_sol"][:, k].astype(np.complex128),
+                     g["adj_rhs"][:, k].astype(np.complex128)) < 1e-5

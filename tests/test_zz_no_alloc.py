@@ -84,3 +84,28 @@ def test_noalloc_rejects_too_many_emitters():
                                        N.stream_handle(torch, dev))
     assert st == N.USV_ERR_TOO_LARGE
     assert "no-allocation" in N.status_string(st)
+
+
+def test_noalloc_against_fp64_host_gradient():
+    """Pinned independently of the workspace entry point: the gradient
+    Re(conj((G^H g)_m) i e^{i phi_m}) and the response G^H g computed on the
+    host in FP64 (numpy) for one complex128 case."""
+    lib = N.load()
+    n, m = 20_011, 16
+    dev, basis, cot, phases = _case(n, m, N.PREC_FP64, seed=7)
+    resp = torch.empty(m, dtype=torch.complex128, device=dev)
+    grad = torch.empty(m, dtype=torch.float64, device=dev)
+    st = lib.usv_basis_adjoint_noalloc(N.ptr(basis), n, m, N.PREC_FP64, N.ptr(cot),
+                                       N.ptr(phases), N.ptr(resp), N.ptr(grad),
+                                       N.stream_handle(torch, dev))
+    assert st == N.USV_OK
+    torch.cuda.synchronize()
+    G = basis.cpu().numpy().T            # (n, m): column m is emitter m
+    g = cot.cpu().numpy()
+    phi = phases.cpu().numpy()
+    resp_host = G.conj().T @ g
+    grad_host = np.real(np.conj(resp_host) * 1j * np.exp(1j * phi))
+    np.testing.assert_allclose(resp.cpu().numpy(), resp_host, rtol=1e-12,
+                               atol=1e-12 * np.abs(resp_host).max())
+    np.testing.assert_allclose(grad.cpu().numpy(), grad_host, rtol=1e-10,
+                               atol=1e-12 * np.abs(grad_host).max())

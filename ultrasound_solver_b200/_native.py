@@ -12,6 +12,7 @@ from pathlib import Path
 
 from . import build as _build
 
+ABI_VERSION = 3
 USV_OK = 0
 USV_ERR_ARG = 1
 USV_ERR_CUDA = 2
@@ -22,6 +23,7 @@ USV_ERR_SOURCE_PML = 6
 USV_ERR_SOURCE_SOFT = 7
 USV_ERR_SOURCE_CLEARANCE = 8
 USV_ERR_TOO_LARGE = 9
+USV_ERR_DEVICE_TIMEOUT = 10
 
 FACE_REFLECTING, FACE_OPEN, FACE_SOFT, FACE_IMPEDANCE = 0, 1, 2, 3
 APPLY_A, APPLY_AH, APPLY_ABS_A, APPLY_ABS_AH, APPLY_K, APPLY_KH = range(6)
@@ -56,7 +58,8 @@ class GmresParams(C.Structure):
                 ("block_nodes", C.c_int32), ("history_capacity", C.c_int32),
                 ("history", C.POINTER(C.c_double)),
                 ("profile", C.POINTER(GmresProfile)),
-                ("recycle", C.c_int32), ("recycle_every", C.c_int32)]
+                ("recycle", C.c_int32), ("recycle_every", C.c_int32),
+                ("max_ctas", C.c_int32), ("reserved", C.c_int32)]
 
 
 class GmresStats(C.Structure):
@@ -125,7 +128,7 @@ def load(path: Path | None = None, build_if_missing: bool = False):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = res
-    if lib.usv_abi_version() != 2:
+    if lib.usv_abi_version() != ABI_VERSION:
         raise RuntimeError("libusv_b200 ABI version mismatch")
     if path is None:
         _lib = lib

@@ -79,12 +79,20 @@ __global__ void k_target(const C2* G, long long nx, long long ny, long long nz, 
         const long long dims[3] = {nx, ny, nz};
         long long lo[3];
         double fr[3];
+        bool finite = true;
         for (int a = 0; a < 3; ++a) {
             const double pos = pts[3 * p + a] / dx;
-            long long l = (long long)floor(pos);
-            if (l > dims[a] - 2) l = dims[a] - 2;
-            lo[a] = l;
-            fr[a] = pos - double(l);
+            finite = finite && isfinite(pos);
+            // the low corner stays in [0, dims-2] (clamped before the integer
+            // conversion): a point outside the grid extrapolates from the edge
+            // cell, a non-finite one gives NaN, and no load leaves G
+            const double l = fmin(fmax(floor(pos), 0.0), double(dims[a] - 2));
+            lo[a] = finite ? (long long)l : 0;
+            fr[a] = pos - l;
+        }
+        if (!finite) {
+            out[t] = make_double2(nan(""), nan(""));
+            continue;
         }
         const long long N = nx * ny * nz;
         double2 acc = make_double2(0.0, 0.0);
@@ -226,7 +234,9 @@ __global__ void __launch_bounds__(256) k_basis_dots_strided(const C2* G, long lo
     if (threadIdx.x == 0) partial[(long long)m * gridDim.x + blockIdx.x] = make_double2(re, im);
 }
 
-// Device address of g_noalloc_partials, resolved once per device.
+// Device address of g_noalloc_partials, resolved once per device and cached
+// for the life of the process; a cudaDeviceReset invalidates the cached
+// address, so this entry point must not be used on a device after a reset.
 static int noalloc_scratch(double2** out) {
     static std::mutex lock;
     static void* addr[256] = {};

@@ -23,6 +23,7 @@
 //            the cycle back-substitutes y.
 // Basis vectors are stored unnormalised with a scale sigma_t = 1/||u_t||.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -32,9 +33,12 @@
 
 #define USV_MAX_RESTART 112  // keeps the m x (m+1) least-squares tile in shared memory
 
+static_assert(sizeof(usv_gmres_params) == 80, "usv_gmres_params layout (include/usv.h)");
+
 namespace usv {
 
-enum { ST_ACTIVE = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_NONFINITE = 3 };
+enum { ST_ACTIVE = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_NONFINITE = 3,
+       ST_DEVICE_TIMEOUT = 4 };  // a bounded device-side wait ran out
 
 // Per-RHS control words of a recycled (GCRO-DR) cycle, written by the host
 // before each cycle.
@@ -757,6 +761,101 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
     return *reinterpret_cast<const float2*>(&d);
 }
 
+// Last CTA of an orthogonalisation launch: beta = ||u_{j+1}|| from the
+// per-CTA partials, then (proj) the start of the Krylov part of a recycled
+// cycle, or the Givens update of Hessenberg column j, the raw column for the
+// harmonic Ritz step and the end-of-cycle flag.
+template <typename C2>
+__device__ __forceinline__ void orth_finish(GState& g, int b, const CycleBasis<C2>& cb, int j, int proj,
+                                         double* sh, double2* hs, double2* gsS, double* gcS) {
+    const int m = g.m;
+    const double beta = sqrt(reduce_slot0(g, b, sh));
+    if (proj) {
+        if (threadIdx.x == 0) {
+            g.counter[b] = 0;
+            const int kc = cb.kc;
+            if (beta > 1e-300 && isfinite(beta)) {
+                g.g[b * (m + 1) + kc] = make_double2(beta, 0.0);
+                g.sigma[b * (m + 1) + kc] = 1.0 / beta;
+            } else {  // r lies in span(C): the projection alone solves this cycle
+                g.g[b * (m + 1) + kc] = make_double2(0.0, 0.0);
+                g.len[b] = kc;
+                g.ended[b] = 1;
+            }
+        }
+        return;
+    }
+    // stage column j and the previous rotations in shared memory
+    double2* col = g.H + ((long long)b * m + j) * (m + 1);
+    for (int t = threadIdx.x; t <= j; t += blockDim.x) {
+        hs[t] = col[t];
+        if (t < j) {
+            gcS[t] = g.gc[(long long)b * m + t];
+            gsS[t] = g.gs[(long long)b * m + t];
+        }
+    }
+    __syncthreads();
+    if (g.kr > 0) {  // raw column of G (before the rotations) for the harmonic Ritz step
+        double* gr = g.hb + (long long)b * g.hb_len + hb_graw(m) + 2LL * j * (m + 1);
+        for (int t = threadIdx.x; t <= j + 1; t += blockDim.x) {
+            const double2 v = t <= j ? hs[t] : make_double2(beta, 0.0);
+            gr[2 * t] = v.x;
+            gr[2 * t + 1] = v.y;
+        }
+    }
+    if (threadIdx.x == 0) {
+        g.counter[b] = 0;
+        hs[j + 1] = make_double2(beta, 0.0);
+        for (int i = 0; i < j; ++i) {
+            const double2 a = hs[i], c2 = hs[i + 1];
+            const double c = gcS[i];
+            const double2 sn = gsS[i];
+            hs[i] = cadd(cscale(a, c), cmul(sn, c2));
+            hs[i + 1] = csub(cscale(c2, c), cmulc(sn, a));
+        }
+        // rotation zeroing beta: c = |a|/r, s = (a/|a|) beta/r, rho = (a/|a|) r
+        const double2 a = hs[j];
+        const double aa = hypot(a.x, a.y);
+        const double r = hypot(aa, beta);
+        double c;
+        double2 sn, rho;
+        if (aa == 0.0) {
+            c = 0.0;
+            sn = make_double2(1.0, 0.0);
+            rho = make_double2(beta, 0.0);
+        } else {
+            c = aa / r;
+            const double2 ph = cscale(a, 1.0 / aa);
+            sn = cscale(ph, beta / r);
+            rho = cscale(ph, r);
+        }
+        hs[j] = rho;
+        gcS[j] = c;
+        gsS[j] = sn;
+        double2* gg = g.g + (long long)b * (m + 1);
+        const double2 gj = gg[j];
+        const double2 gn = make_double2(-(sn.x * gj.x + sn.y * gj.y), -(sn.x * gj.y - sn.y * gj.x));
+        gg[j + 1] = gn;
+        gg[j] = cscale(gj, c);
+        const bool nonfinite = !isfinite(beta);
+        const bool breakdown = !(beta > 1e-30 * g.wnorm[b]);
+        g.sigma[b * (m + 1) + j + 1] = (breakdown || nonfinite) ? 0.0 : 1.0 / beta;
+        const double resid = hypot(gn.x, gn.y);
+        const bool end = (j == m - 1) || breakdown || nonfinite ||
+                         (!g.full_cycles && resid <= g.atol[b]);
+        if (end) {
+            g.len[b] = j + 1;
+            g.ended[b] = 1;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t <= j; t += blockDim.x) col[t] = hs[t];
+    if (threadIdx.x == 0) {
+        g.gc[(long long)b * m + j] = gcS[j];
+        g.gs[(long long)b * m + j] = gsS[j];
+    }
+}
+
 // ------------------------------------------------------------ Arnoldi: orthogonalise + norm
 // proj = 1 (recycled cycles): r -= sum_t alpha_t C_t on the cycle's first
 // residual (slot kc), then beta = ||r|| starts the Krylov part of the cycle.
@@ -840,91 +939,202 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     if (threadIdx.x == 0)
         g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    const double beta = sqrt(reduce_slot0(g, b, sh));
-    if (proj) {
-        if (threadIdx.x == 0) {
-            g.counter[b] = 0;
-            const int kc = cb.kc;
-            if (beta > 1e-300 && isfinite(beta)) {
-                g.g[b * (m + 1) + kc] = make_double2(beta, 0.0);
-                g.sigma[b * (m + 1) + kc] = 1.0 / beta;
-            } else {  // r lies in span(C): the projection alone solves this cycle
-                g.g[b * (m + 1) + kc] = make_double2(0.0, 0.0);
-                g.len[b] = kc;
-                g.ended[b] = 1;
-            }
+    orth_finish<C2>(g, b, cb, j, proj, sh, hs, gsS, gcS);
+}
+
+// Bulk-copy form of k_orth: the basis tiles reach shared memory by
+// cp.async.bulk (one instruction per chunk tile instead of a 16-byte cp.async
+// per thread and unit), issued by one producer thread kOrthStages - 1 tiles
+// ahead through a ring of full / empty mbarriers; 256 consumer threads keep
+// the node mapping and arithmetic of k_orth. Per chunk the tiles are w (slot
+// j+1) then u_0 .. u_j. Every wait is bounded: when one runs out the RHS ends
+// with ST_DEVICE_TIMEOUT, the producer waits (bounded) for the copies it has
+// in flight, and the CTA leaves.
+template <typename S> struct OrthBulk {
+    static constexpr int TILE = kChunk * int(sizeof(S));   // bytes per chunk tile
+    static constexpr int STAGES = sizeof(S) == 4 ? 6 : (sizeof(S) == 8 ? 4 : 3);
+    static constexpr size_t SMEM = size_t(STAGES) * TILE + 2 * STAGES * sizeof(unsigned long long);
+    static constexpr int THREADS = kThreads + 32;           // + the producer warp
+};
+
+// values of this thread's pairs from a chunk tile (nodes >= len read as zero)
+template <typename C2, typename M2>
+__device__ __forceinline__ void tile_pairs(const char* tile, int len, M2 (&v)[kPairs][2]) {
+    if constexpr (std::is_same<C2, bf2>::value) {
+#pragma unroll
+        for (int u = 0; u < kPairs / 2; ++u) {
+            const int e = 4 * (threadIdx.x + kThreads * u);
+            const uint4 raw = reinterpret_cast<const uint4*>(tile)[threadIdx.x + kThreads * u];
+            const unsigned w4[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                v[2 * u + c / 2][c % 2] = e + c < len ? to_f(*reinterpret_cast<const bf2*>(&w4[c]))
+                                                      : cmake<M2>(0.0, 0.0);
         }
+    } else if constexpr (std::is_same<C2, float2>::value) {
+#pragma unroll
+        for (int k = 0; k < kPairs; ++k) {
+            const int e = pair_node<C2>(k);
+            const float4 r = reinterpret_cast<const float4*>(tile)[threadIdx.x + kThreads * k];
+            v[k][0] = e < len ? make_double2(r.x, r.y) : make_double2(0.0, 0.0);
+            v[k][1] = e + 1 < len ? make_double2(r.z, r.w) : make_double2(0.0, 0.0);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPairs; ++k) {
+            const int e = pair_node<C2>(k);
+            const double2* d = reinterpret_cast<const double2*>(tile) + e;
+            v[k][0] = e < len ? d[0] : make_double2(0.0, 0.0);
+            v[k][1] = e + 1 < len ? d[1] : make_double2(0.0, 0.0);
+        }
+    }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long long N, GState g,
+                                                                   int j, int proj) {
+    using C2 = S;
+    using P = OrthBulk<S>;
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    if (proj) {
+        if (cb.kc == 0) return;
+        j = cb.kc - 1;
+    } else if (j < cb.kc) {
         return;
     }
-    // stage column j and the previous rotations in shared memory
-    double2* col = g.H + ((long long)b * m + j) * (m + 1);
-    for (int t = threadIdx.x; t <= j; t += kThreads) {
-        hs[t] = col[t];
-        if (t < j) {
-            gcS[t] = g.gc[(long long)b * m + t];
-            gsS[t] = g.gs[(long long)b * m + t];
-        }
-    }
-    __syncthreads();
-    if (g.kr > 0) {  // raw column of G (before the rotations) for the harmonic Ritz step
-        double* gr = g.hb + (long long)b * g.hb_len + hb_graw(m) + 2LL * j * (m + 1);
-        for (int t = threadIdx.x; t <= j + 1; t += kThreads) {
-            const double2 v = t <= j ? hs[t] : make_double2(beta, 0.0);
-            gr[2 * t] = v.x;
-            gr[2 * t + 1] = v.y;
-        }
+    extern __shared__ __align__(128) char ring[];
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(ring + size_t(P::STAGES) * P::TILE);
+    unsigned long long* empty = full + P::STAGES;
+    __shared__ double2 hs[USV_MAX_RESTART + 2];
+    __shared__ double2 gsS[USV_MAX_RESTART + 1];
+    __shared__ double gcS[USV_MAX_RESTART + 1];
+    __shared__ double sh[32];
+    __shared__ int failed;
+    using M2 = typename MathT<C2>::T2;
+    __shared__ M2 hm[USV_MAX_RESTART + 2];
+    const int m = g.m;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = threadIdx.x; t <= j; t += blockDim.x) {
+        hs[t] = proj ? g.alpha[(long long)b * g.kr + t]
+                     : cscale(g.H[((long long)b * m + j) * (m + 1) + t], g.sigma[b * (m + 1) + t]);
+        hm[t] = cmake<M2>(hs[t].x, hs[t].y);
     }
     if (threadIdx.x == 0) {
-        g.counter[b] = 0;
-        hs[j + 1] = make_double2(beta, 0.0);
-        for (int i = 0; i < j; ++i) {
-            const double2 a = hs[i], c2 = hs[i + 1];
-            const double c = gcS[i];
-            const double2 sn = gsS[i];
-            hs[i] = cadd(cscale(a, c), cmul(sn, c2));
-            hs[i + 1] = csub(cscale(c2, c), cmulc(sn, a));
+        failed = 0;
+        for (int s = 0; s < P::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kThreads / 32);
         }
-        // rotation zeroing beta: c = |a|/r, s = (a/|a|) beta/r, rho = (a/|a|) r
-        const double2 a = hs[j];
-        const double aa = hypot(a.x, a.y);
-        const double r = hypot(aa, beta);
-        double c;
-        double2 sn, rho;
-        if (aa == 0.0) {
-            c = 0.0;
-            sn = make_double2(1.0, 0.0);
-            rho = make_double2(beta, 0.0);
-        } else {
-            c = aa / r;
-            const double2 ph = cscale(a, 1.0 / aa);
-            sn = cscale(ph, beta / r);
-            rho = cscale(ph, r);
+        mbar_fence_init();
+    }
+    __syncthreads();  // hs, hm, barriers visible
+    const int tpc = j + 2;  // tiles per chunk: w, u_0 .. u_j
+    const int nmy = int((g.nchunk - blockIdx.x + gridDim.x - 1) / gridDim.x);
+    double acc = 0.0;
+    if (warp == kThreads / 32) {
+        // producer: one elected thread issues every tile of this CTA in order
+        if (lane == 0) {
+            long long q = 0;
+            bool ok = true;
+            for (int i = 0; i < nmy && ok; ++i) {
+                const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
+                const int len = int(min((long long)kChunk, N - n0));
+                const unsigned bytes = unsigned((size_t(len) * sizeof(C2) + 15) / 16 * 16);
+                for (int tt = 0; tt < tpc; ++tt, ++q) {
+                    const int s = int(q % P::STAGES);
+                    if (!mbar_wait(&empty[s], unsigned((q / P::STAGES) & 1) ^ 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    const C2* src = tt == 0 ? cb.V + (long long)(j + 1) * g.nv + n0
+                                            : (tt - 1 < cb.kc ? cb.C : cb.V) +
+                                                  (long long)(tt - 1) * g.nv + n0;
+                    mbar_expect_tx(&full[s], bytes);
+                    bulk_g2s(ring + size_t(s) * P::TILE, src, bytes, &full[s]);
+                }
+            }
+            if (!ok) {
+                failed = 1;
+                g.status[b] = ST_DEVICE_TIMEOUT;
+            }
+            // copies still in flight (none unless a wait ran out): the last
+            // tile issued on each stage must land before the CTA leaves
+            for (long long r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
+                mbar_wait(&full[r % P::STAGES], unsigned((r / P::STAGES) & 1));
         }
-        hs[j] = rho;
-        gcS[j] = c;
-        gsS[j] = sn;
-        double2* gg = g.g + (long long)b * (m + 1);
-        const double2 gj = gg[j];
-        const double2 gn = make_double2(-(sn.x * gj.x + sn.y * gj.y), -(sn.x * gj.y - sn.y * gj.x));
-        gg[j + 1] = gn;
-        gg[j] = cscale(gj, c);
-        const bool nonfinite = !isfinite(beta);
-        const bool breakdown = !(beta > 1e-30 * g.wnorm[b]);
-        g.sigma[b * (m + 1) + j + 1] = (breakdown || nonfinite) ? 0.0 : 1.0 / beta;
-        const double resid = hypot(gn.x, gn.y);
-        const bool end = (j == m - 1) || breakdown || nonfinite ||
-                         (!g.full_cycles && resid <= g.atol[b]);
-        if (end) {
-            g.len[b] = j + 1;
-            g.ended[b] = 1;
+    } else {
+        long long q = 0;
+        for (int i = 0; i < nmy; ++i) {
+            const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
+            const int len = int(min((long long)kChunk, N - n0));
+            M2 u[kPairs][2];
+            float2 qacc[kPairs][2];  // bfloat16: the (Im, Re) half of the packed products
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k) qacc[k][0] = qacc[k][1] = make_float2(0.f, 0.f);
+            bool ok = true;
+            for (int tt = 0; tt < tpc; ++tt, ++q) {
+                const int s = int(q % P::STAGES);
+                if (!mbar_wait(&full[s], unsigned((q / P::STAGES) & 1))) {
+                    ok = false;
+                    break;
+                }
+                M2 v[kPairs][2];
+                tile_pairs<C2>(ring + size_t(s) * P::TILE, len, v);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[s]);
+                if (tt == 0) {
+#pragma unroll
+                    for (int k = 0; k < kPairs; ++k) u[k][0] = v[k][0], u[k][1] = v[k][1];
+                    continue;
+                }
+                const M2 h = hm[tt - 1];
+#pragma unroll
+                for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        if constexpr (std::is_same<C2, bf2>::value) {
+                            u[k][c] = ffma2(v[k][c], make_float2(-h.x, -h.x), u[k][c]);
+                            qacc[k][c] = ffma2(v[k][c], make_float2(-h.y, h.y), qacc[k][c]);
+                        } else {
+                            u[k][c].x -= h.x * v[k][c].x - h.y * v[k][c].y;
+                            u[k][c].y -= h.x * v[k][c].y + h.y * v[k][c].x;
+                        }
+                    }
+            }
+            if (!ok) {
+                failed = 1;
+                g.status[b] = ST_DEVICE_TIMEOUT;
+                break;
+            }
+            if constexpr (std::is_same<C2, bf2>::value) {
+#pragma unroll
+                for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        u[k][c].x += qacc[k][c].y;
+                        u[k][c].y += qacc[k][c].x;
+                    }
+            }
+            C2* w = cb.V + (long long)(j + 1) * g.nv + n0;
+#pragma unroll
+            for (int k = 0; k < kPairs; ++k) {
+                const int e = pair_node<C2>(k);
+                if (e < len) {
+                    st_pair(w + e, u[k][0], u[k][1]);
+                    acc += double(cabs2(rounded(w, u[k][0])));
+                    if (e + 1 < len) acc += double(cabs2(rounded(w, u[k][1])));
+                }
+            }
         }
     }
-    __syncthreads();
-    for (int t = threadIdx.x; t <= j; t += kThreads) col[t] = hs[t];
-    if (threadIdx.x == 0) {
-        g.gc[(long long)b * m + j] = gcS[j];
-        g.gs[(long long)b * m + j] = gsS[j];
-    }
+    acc = block_sum(acc, sh);
+    if (failed) return;
+    if (threadIdx.x == 0)
+        g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    orth_finish<C2>(g, b, cb, j, proj, sh, hs, gsS, gcS);
 }
 
 // ------------------------------------------------------------ least squares (once per cycle)
@@ -1564,17 +1774,43 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
 }
 
 // ------------------------------------------------------------ host driver
-static cudaStream_t capture_stream() {
-    static thread_local cudaStream_t s = nullptr;
-    static thread_local int dev = -1;
+// A private stream per (host thread, device) for the graph capture, created
+// on first use and kept for the life of the thread.
+static cudaError_t capture_stream(cudaStream_t* out) {
+    constexpr int kMaxDevices = 64;
+    static thread_local cudaStream_t streams[kMaxDevices] = {};
     int cur = 0;
-    cudaGetDevice(&cur);
-    if (s == nullptr || dev != cur) {
-        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-        dev = cur;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return e;
+    if (cur < 0 || cur >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (streams[cur] == nullptr) {
+        e = cudaStreamCreateWithFlags(&streams[cur], cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            streams[cur] = nullptr;
+            return e;
+        }
     }
-    return s;
+    *out = streams[cur];
+    return cudaSuccess;
 }
+
+// Owners of the per-solve graph and timing events: every return path of the
+// driver releases them.
+struct GraphHold {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~GraphHold() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+struct EventHold {
+    std::vector<cudaEvent_t> v;
+    ~EventHold() {
+        for (cudaEvent_t e : v)
+            if (e) cudaEventDestroy(e);
+    }
+};
 
 
 // The recycled-space kernels are instantiated for every k = 1..kMaxRecycle.
@@ -1693,6 +1929,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         int per_sm = 0;
         USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
         long long x = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1) / B;
+        if (p.max_ctas > 0 && x > p.max_ctas) x = p.max_ctas;
         x = x < 1 ? 1 : (x > g.nchunk ? g.nchunk : x);
         grid = dim3(unsigned(x), unsigned(B));
         return USV_OK;
@@ -1704,7 +1941,25 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     auto launch_dots = [&](cudaStream_t st, int j, int proj) {
         k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
     };
-    if (int e = grid_for((const void*)k_orth<S>, kThreads, pipe_smem, grid_orth)) return e;
+    // orthogonalisation kernel: the bulk-copy ring (default) or the per-thread
+    // cp.async pipeline (USV_ORTH_KERNEL=cpasync)
+    static const bool orth_cpasync = [] {
+        const char* v = getenv("USV_ORTH_KERNEL");
+        return v && std::strcmp(v, "cpasync") == 0;
+    }();
+    const void* fn_orth = orth_cpasync ? (const void*)k_orth<S> : (const void*)k_orth_bulk<S>;
+    const int orth_threads = orth_cpasync ? kThreads : OrthBulk<S>::THREADS;
+    const size_t orth_smem = orth_cpasync ? pipe_smem : OrthBulk<S>::SMEM;
+    USV_CUDA_TRY(cudaFuncSetAttribute(fn_orth, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(orth_smem)));
+    if (int e = grid_for(fn_orth, orth_threads, orth_smem, grid_orth)) return e;
+    auto launch_orth = [&](cudaStream_t st, int j, int proj) -> cudaError_t {
+        C2* vp = V;
+        long long nn_ = g.n;
+        GState gs = g;
+        void* args[] = {&vp, &nn_, &gs, &j, &proj};
+        return cudaLaunchKernel(fn_orth, grid_orth, dim3(orth_threads), args, orth_smem, st);
+    };
     if (int e = grid_for((const void*)k_update<S>, kThreads, pipe_smem, grid_upd)) return e;
     if (int e = grid_for((const void*)k_gates<ADJ>, 256, 0, grid_gates)) return e;
     if (lsq_smem > 48 * 1024)
@@ -1767,10 +2022,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     // every kernel; consecutive pairs bracket single launches.
     usv_gmres_profile* prof = p.profile;
     const int kernels_per_cycle = 2 * g.m + 3 + (kr > 0 ? 3 : 0);
-    std::vector<cudaEvent_t> ev;
+    EventHold events;
+    std::vector<cudaEvent_t>& ev = events.v;
     std::vector<int> fam;
     if (prof) {
-        ev.resize(kernels_per_cycle + 1);
+        ev.assign(kernels_per_cycle + 1, nullptr);
         for (auto& e : ev) USV_CUDA_TRY(cudaEventCreate(&e));
     }
     const double vb = double(sizeof(C2)), nn = double(g.n);
@@ -1819,7 +2075,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam_step.push_back(-1);
             fam_need.push_back(0);
             launch_dots(st, 0, 1);
-            k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, 0, 1);
+            USV_CUDA_TRY(launch_orth(st, 0, 1));
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(7);
             fam_bytes.push_back(nn * vb * (2.0 * kr + 3));
@@ -1838,7 +2094,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam_shared.push_back(nn * (sizeof(R) == 4 ? 48.0 : 32.0));
             fam_step.push_back(j);
             fam_need.push_back(0);
-            k_orth<S><<<grid_orth, kThreads, pipe_smem, st>>>(V, g.n, g, j, 0);
+            USV_CUDA_TRY(launch_orth(st, j, 0));
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(1);
             fam_bytes.push_back(nn * vb * (j + 3));
@@ -1909,16 +2165,17 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         return USV_OK;
     };
 
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
+    GraphHold cycle_graph;
+    cudaGraphExec_t& exec = cycle_graph.exec;
     if (p.use_graph) {
-        cudaStream_t cap = capture_stream();
+        cudaStream_t cap = nullptr;
+        USV_CUDA_TRY(capture_stream(&cap));
         USV_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
         int st = launch_cycle(cap, true);
-        cudaError_t e = cudaStreamEndCapture(cap, &graph);
+        cudaError_t e = cudaStreamEndCapture(cap, &cycle_graph.graph);
         if (st) return st;
         USV_CUDA_TRY(e);
-        USV_CUDA_TRY(cudaGraphInstantiate(&exec, graph, 0));
+        USV_CUDA_TRY(cudaGraphInstantiate(&exec, cycle_graph.graph, 0));
     }
     std::vector<int> status(B);
     std::vector<int> active(1, 0);
@@ -2020,12 +2277,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
                                     pend[b].src_kc == before[b].kc;
         }
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    if (rc) {
-        for (auto& e : ev) cudaEventDestroy(e);
-        return rc;
-    }
+    if (rc) return rc;
     if (prof) USV_CUDA_TRY(cudaEventRecord(ev[0], strm));
     k_gates<ADJ><<<grid_gates, 256, 0, strm>>>(op64, rhs, x, ld, g);
     USV_CUDA_TRY(cudaGetLastError());
@@ -2037,7 +2289,6 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         prof->milliseconds[5] += ms;
         prof->launches[5] += 1;
         prof->bytes[5] += nn * B * (2 * sizeof(double2) + sizeof(double4) + sizeof(double2));
-        for (auto& e : ev) cudaEventDestroy(e);
     }
     std::vector<double> gates(4 * B);
     std::vector<int> cycles(B), iters(B);
@@ -2064,7 +2315,8 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         // CuPy reports info = iterations only when the cap was hit exactly
         st.info = (status[b] != ST_CONVERGED && iters[b] == p.maxiter) ? iters[b] : 0;
         const bool finite = gates[4 * b + 2] == 0.0;
-        if (!finite || status[b] == ST_NONFINITE) st.status = USV_ERR_NONFINITE;
+        if (status[b] == ST_DEVICE_TIMEOUT) st.status = USV_ERR_DEVICE_TIMEOUT;
+        else if (!finite || status[b] == ST_NONFINITE) st.status = USV_ERR_NONFINITE;
         else if (st.info != 0 || status[b] != ST_CONVERGED || !(st.scaled_residual <= p.rtol) ||
                  !(st.backward_error <= p.backward_error_tol))
             st.status = USV_ERR_NOT_CONVERGED;

@@ -395,6 +395,7 @@ const char* usv_status_string(int status) {
             return "Sinc aperture needs one grid cell clearance from side boundaries";
         case USV_ERR_TOO_LARGE:
             return "size exceeds the fixed maximum of the no-allocation entry point";
+        case USV_ERR_DEVICE_TIMEOUT: return "a bounded device-side wait ran out";
         default: return "unknown status";
     }
 }

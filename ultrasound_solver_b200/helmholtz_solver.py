@@ -41,6 +41,69 @@ def _as_dict(obj):
     return asdict(obj) if is_dataclass(obj) else dict(vars(obj))
 
 
+def _array_record(array) -> bytes:
+    a = np.ascontiguousarray(array)
+    return f"{a.dtype.str}{a.shape}".encode() + a.tobytes()
+
+
+def _digest_records(records) -> str:
+    """BLAKE2b over (label, payload) records, each length-prefixed."""
+    h = hashlib.blake2b(digest_size=32)
+    for label, payload in records:
+        tag = label.encode()
+        h.update(len(tag).to_bytes(4, "little") + tag)
+        h.update(len(payload).to_bytes(8, "little"))
+        h.update(payload)
+    return h.hexdigest()
+
+
+class _ResponseStore:
+    """Target responses kept in one .npz file, valid for one cache key.
+
+    Points are matched on a 1 nm lattice (their coordinates rounded to
+    integer nanometres); entries written for another key are ignored and
+    replaced on the next write. Writes go to a temporary file that is then
+    renamed over the store.
+    """
+
+    def __init__(self, path: Path, key: str, channels: int):
+        self.path, self.key, self.channels = path, key, channels
+        self.points = np.empty((0, 3))
+        self.values = np.empty((0, channels), complex)
+        try:
+            with np.load(path, allow_pickle=False) as data:
+                if str(data["key"]) == key:
+                    pts, vals = np.asarray(data["points"], float), np.asarray(data["values"])
+                    if (pts.ndim == 2 and pts.shape[1] == 3 and vals.shape == (len(pts), channels)
+                            and np.isfinite(pts).all() and np.isfinite(vals).all()):
+                        self.points, self.values = pts, vals.astype(complex)
+        except (OSError, KeyError, ValueError):
+            pass
+
+    @staticmethod
+    def _lattice(points):
+        return [tuple(r) for r in np.rint(np.asarray(points) * 1e9).astype(np.int64)]
+
+    def lookup(self, points, out) -> np.ndarray:
+        """Fill out[i] for stored points; returns the mask of points found."""
+        index = {k: i for i, k in enumerate(self._lattice(self.points))}
+        found = np.zeros(len(points), bool)
+        for i, k in enumerate(self._lattice(points)):
+            j = index.get(k)
+            if j is not None:
+                out[i] = self.values[j]
+                found[i] = True
+        return found
+
+    def add(self, points, values):
+        self.points = np.vstack((self.points, points))
+        self.values = np.vstack((self.values, values))
+        self.path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = self.path.with_name(self.path.name + ".partial.npz")
+        np.savez_compressed(tmp, key=self.key, points=self.points, values=self.values)
+        tmp.replace(self.path)
+
+
 class HelmholtzB200Solver:
     """Assemble and solve the discrete Helmholtz system on one B200."""
 
@@ -81,6 +144,7 @@ class HelmholtzB200Solver:
             recycle=int(s.get("gmres_recycle", 0)),
             recycle_every=int(s.get("gmres_recycle_every", 1)),
             batch_width=int(s.get("gmres_batch_width", 0)),
+            max_ctas=int(s.get("gmres_max_ctas", 0)),
         )
 
     # ----------------------------------------------------------- scene
@@ -104,31 +168,37 @@ class HelmholtzB200Solver:
         self.invalidate_factorization()
 
     def scene_fingerprint(self):
-        """Hash of every matrix-defining input (helmholtz_solver.py:249-271)."""
+        """Digest of every input that defines the matrix and the sources.
+
+        The reference keys cached factorizations and stored bases on such a
+        digest (helmholtz_solver.py:249-271); this one is built as a sequence
+        of labelled, length-prefixed records (the scene description as
+        canonical JSON, then each array input with its dtype and shape, then
+        each referenced file), so two scenes share a fingerprint only if every
+        record matches.
+        """
         if (_as_dict(self.cfg.domain) != self._grid_definition
                 or _as_dict(self.cfg.specs) != self._source_definition):
             raise ValueError("Grid or source specification changed; construct a new solver")
-        files = [o["file"] for o in self.cfg.obstacles if o.get("type", "").lower() == "mesh"]
-        if self.cfg.physics.material_field_file:
-            files.append(self.cfg.physics.material_field_file)
-        digest = hashlib.sha256(json.dumps({
+        description = {
             "model": self.MODEL_VERSION, "physics": _as_dict(self.cfg.physics),
             "domain": _as_dict(self.cfg.domain), "specs": _as_dict(self.cfg.specs),
-            "origin_m": self.origin.tolist(),
-            "centers": (self.transducers.centers - self.origin).tolist(),
             "boundaries": self.cfg.boundary_conditions, "obstacles": self.cfg.obstacles,
             "pml": self.cfg.solver.get("pml", {}),
-        }, sort_keys=True).encode())
-        for filename in files:
-            with Path(filename).open("rb") as stream:
-                for chunk in iter(lambda: stream.read(1024 * 1024), b""):
-                    digest.update(chunk)
+            "source_centres_from_origin": (self.transducers.centers - self.origin).tolist()}
+        records = [("scene", json.dumps(description, sort_keys=True, default=str).encode())]
         if self._material_fields is not None:
-            for array in self._material_fields:
-                digest.update(array.tobytes())
+            records += [(f"material[{i}]", _array_record(a))
+                        for i, a in enumerate(self._material_fields)]
         if self._obs_sdf is not None:
-            digest.update(self._obs_sdf.tobytes())
-        return digest.hexdigest()
+            records.append(("obstacle_sdf", _array_record(self._obs_sdf)))
+        referenced = [o["file"] for o in self.cfg.obstacles
+                      if o.get("type", "").lower() == "mesh"]
+        if self.cfg.physics.material_field_file:
+            referenced.append(self.cfg.physics.material_field_file)
+        for name in referenced:
+            records.append((f"file:{Path(name).name}", Path(name).read_bytes()))
+        return _digest_records(records)
 
     def source_diagnostics(self):
         centers = (self.transducers.centers - self.origin)[:, :2]
@@ -281,70 +351,34 @@ class HelmholtzB200Solver:
                     raise ValueError("Target lies in PML; enlarge the physical interior")
         return local
 
-    def _target_response_cache_fingerprint(self):
-        digest = hashlib.sha256()
-        here = Path(__file__)
-        for path in (here, here.with_name("homogeneous_surface.py"), here.with_name("scene.py")):
-            digest.update(path.read_bytes())
-        payload = {"model": self.MODEL_VERSION, "scene": self.scene_fingerprint(),
-                   "origin_m": self.origin.tolist(), "implementation_sha256": digest.hexdigest()}
-        return hashlib.sha256(json.dumps(payload, sort_keys=True,
-                                         separators=(",", ":")).encode()).hexdigest()
-
-    def _read_target_response_cache(self):
+    def _target_response_cache(self):
+        """The optional on-disk store of computed target responses
+        (solver.target_response_cache), keyed to this scene and to the code
+        that computes the responses."""
         filename = str(self.cfg.solver.get("target_response_cache", "")).strip()
-        path = Path(filename) if filename else None
-        if path is None or not path.is_file():
-            return path, None
-        try:
-            with np.load(path, allow_pickle=False) as data:
-                if str(data["fingerprint"]) != self._target_response_cache_fingerprint():
-                    return path, None
-                points = np.asarray(data["points_m"], dtype=float)
-                response = np.asarray(data["response"], dtype=complex)
-        except (KeyError, OSError, ValueError):
-            return path, None
-        if (points.ndim != 2 or points.shape[1] != 3
-                or response.shape != (len(points), self.transducers.num_transducers)
-                or not np.isfinite(points).all() or not np.isfinite(response).all()):
-            return path, None
-        return path, (points, response)
-
-    def _write_target_response_cache(self, path, points, response):
-        if path is None:
-            return
-        path.parent.mkdir(parents=True, exist_ok=True)
-        tmp = path.with_suffix(".tmp.npz")
-        np.savez_compressed(tmp, fingerprint=self._target_response_cache_fingerprint(),
-                            points_m=points, response=response)
-        tmp.replace(path)
+        if not filename:
+            return None
+        here = Path(__file__)
+        code = [(f.name, f.read_bytes()) for f in
+                (here, here.with_name("homogeneous_surface.py"), here.with_name("scene.py"))]
+        key = _digest_records([("scene", self.scene_fingerprint().encode()),
+                               ("origin", self.origin.tobytes()), *code])
+        return _ResponseStore(Path(filename), key, self.transducers.num_transducers)
 
     def target_response(self, points):
         """(P, M) target x channel responses of the discrete PDE (homogeneous scenes)."""
         points = np.asarray(points, dtype=float)
         local = self._local_target_points(points)
-        path, cached = self._read_target_response_cache()
-        channels = self.transducers.num_transducers
-        result = np.empty((len(points), channels), complex)
-        if cached is None:
-            cached_points = np.empty((0, 3), float)
-            cached_response = np.empty((0, channels), complex)
-        else:
-            cached_points, cached_response = cached
-        missing = []
-        for index, point in enumerate(points):
-            hit = np.flatnonzero(np.all(np.isclose(cached_points, point, rtol=0, atol=1e-12), axis=1))
-            if hit.size:
-                result[index] = cached_response[hit[0]]
-            else:
-                missing.append(index)
-        if missing:
+        store = self._target_response_cache()
+        result = np.empty((len(points), self.transducers.num_transducers), complex)
+        found = store.lookup(points, result) if store else np.zeros(len(points), bool)
+        todo = np.flatnonzero(~found)
+        if todo.size:
             self._ensure_target_surface_solver()
-            computed = self._target_surface_solver.flux_target_response(
-                self._target_source_masses, local[missing])
-            result[missing] = computed
-            self._write_target_response_cache(path, np.vstack((cached_points, points[missing])),
-                                              np.vstack((cached_response, computed)))
+            result[todo] = self._target_surface_solver.flux_target_response(
+                self._target_source_masses, local[todo])
+            if store:
+                store.add(points[todo], result[todo])
         return result
 
     def field_at(self, points, phases=None):

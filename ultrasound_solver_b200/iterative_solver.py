@@ -42,7 +42,7 @@ class B200IterativeSolver:
                  backward_error_tol: float = 1.0e-4, precision: str = "mixed",
                  full_cycles: bool = True, use_graph: bool = True, block_nodes: int = 0,
                  verbose: bool = False, profile: bool = False, recycle: int = 0,
-                 recycle_every: int = 1, batch_width: int = 0):
+                 recycle_every: int = 1, batch_width: int = 0, max_ctas: int = 0):
         if str(precision).lower() not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         self.restart = int(restart)
@@ -57,6 +57,9 @@ class B200IterativeSolver:
         self.recycle_every = int(recycle_every)
         # right-hand sides per launch (0: all of them); autotune.BatchTuner picks it
         self.batch_width = int(batch_width)
+        # cap on CTAs per right-hand side (0: fill the GPU); a small cap makes
+        # every CTA of the streaming kernels loop over several node chunks
+        self.max_ctas = int(max_ctas)
         self.verbose = bool(verbose)
         self.profile = bool(profile)
         self.last_profile = None
@@ -81,6 +84,7 @@ class B200IterativeSolver:
         p.history_capacity = self.history_capacity()
         p.recycle = self.recycle
         p.recycle_every = self.recycle_every
+        p.max_ctas = self.max_ctas
         return p
 
     def workspace_bytes(self, operator, nrhs: int, adjoint: bool = False) -> int:

@@ -92,6 +92,69 @@ def config3(n=128, h=1e-3):
     return config1(n, h, array_n=16)
 
 
+def random_rotation(seed):
+    """Uniformly random rotation matrix (QR of a seeded Gaussian matrix)."""
+    rng = np.random.default_rng(seed)
+    q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+    q = q * np.sign(np.diag(r))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    return q
+
+
+def ellipsoid_sdf(shape, h, centre, semi_axes, rotation):
+    """Signed distance (m, Fortran-ordered grid) of a rotated ellipsoid.
+
+    The ellipsoid has no closed-form distance; this is the first-order
+    estimate f = (|q/a| - 1) |q/a| / |q/a^2| in the body frame q = R^T (x - c),
+    exact on the surface, negative inside, within a few per cent of the true
+    distance over the few cells of the material blend."""
+    grids = np.meshgrid(*(np.arange(n) * h for n in shape), indexing="ij")
+    x = np.stack([g - c for g, c in zip(grids, centre)], axis=-1)
+    q = x @ np.asarray(rotation)          # body-frame coordinates (R^T x per point)
+    a = np.asarray(semi_axes, float)
+    k0 = np.linalg.norm(q / a, axis=-1)
+    k1 = np.linalg.norm(q / a ** 2, axis=-1)
+    return np.where(k1 > 0, (k0 - 1.0) * k0 / np.maximum(k1, 1e-300), -float(a.min()))
+
+
+def config4(n=256, h=0.8e-3, array_n=16, seed=2):
+    """Full phase optimisation scene: config-1 medium statistics on an n^3 grid
+    at h, a randomly rotated rigid ellipsoid (semi-axes 45 x 20 x 10 mm at
+    256^3 / 0.8 mm, scaled with the box on smaller grids) blended as a
+    rho = 1250 / c = 2200 obstacle, +x reflecting, -y impedance Z = 2 rho0 c0,
+    the other open faces with the 10-cell PML, an n_a x n_a array and two
+    focal-pressure targets. The ellipsoid enters as a precomputed SDF
+    (obstacle type "sdf"): pass `config4_sdf(cfg)` to build_solver."""
+    L = (n - 1) * h
+    scale = L / (255 * 0.8e-3)
+    p, d = fit_array(array_n, n, h)
+    centre = L / 2
+    targets = [(centre - 0.1 * L, centre, 0.6 * L), (centre + 0.1 * L, centre, 0.6 * L)]
+    obstacle = {"type": "sdf", "smoothing_width_cells": 1.2,
+                "material": {"density": 1250.0, "sound_speed": 2200.0},
+                "center": [centre, centre, 0.35 * L],
+                "semi_axes": [0.045 * scale, 0.020 * scale, 0.010 * scale],
+                "rotation_seed": seed}
+    cfg = scene_dict(n, h, array_n, p, d,
+                     boundaries={"+x": "reflecting",
+                                 "-y": {"type": "impedance",
+                                        "impedance": [2 * RHO_AIR * C_AIR, 0.0]}},
+                     obstacle=obstacle, targets=targets,
+                     solver={"gmres_restart": 30, "precision": "mixed"})
+    cfg["training"].update({"target_weight": 1.0, "background_weight": 0.05})
+    return cfg
+
+
+def config4_sdf(cfg):
+    """The ellipsoid SDF of a config4 scene dict."""
+    ob = cfg["obstacles"][0]
+    shape = tuple(cfg["domain"]["grid_size"])
+    h = cfg["domain"]["box_size"][0] / (shape[0] - 1)
+    return ellipsoid_sdf(shape, h, ob["center"], ob["semi_axes"],
+                         random_rotation(ob["rotation_seed"]))
+
+
 def config2_basis_scene(n=96, h=1e-3):
     """Config-2 basis scene: config-1 medium statistics, 16x16 array (10.5 mm pitch if it fits)."""
     p, d = fit_array(16, n, h)
@@ -124,8 +187,10 @@ def config2_scene_batch(count=32, seed=3, sizes=(48, 64, 80, 96, 112), h=1e-3):
     return out
 
 
-def build_solver(cfg_dict, seed=0, device=None, random=True):
-    """HelmholtzB200Solver for a scene dict; the obstacle is blended into the random medium."""
+def build_solver(cfg_dict, seed=0, device=None, random=True, sdf=None):
+    """HelmholtzB200Solver for a scene dict; the obstacle is blended into the
+    random medium (a sphere from its centre and radius, an "sdf" obstacle from
+    the precomputed `sdf` array)."""
     import torch
 
     from .config import SimulationConfig
@@ -147,7 +212,7 @@ def build_solver(cfg_dict, seed=0, device=None, random=True):
             rho_t, c_t = blend_materials(shape, cfg.domain.dx, dev, obstacle,
                                          cfg.physics.medium_density, cfg.physics.sound_speed,
                                          rho_medium=fortran_flat(rho_m, dev),
-                                         c_medium=fortran_flat(c_m, dev))
+                                         c_medium=fortran_flat(c_m, dev), sdf=sdf)
             rho_m = rho_t.cpu().numpy().reshape(shape, order="F")
             c_m = c_t.cpu().numpy().reshape(shape, order="F")
             torch.cuda.synchronize()
