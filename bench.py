@@ -86,6 +86,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-gradient timing")
     ap.add_argument("--no-stencil", action="store_true", help="skip the stencil-only timing")
     ap.add_argument("--cpu-iters", type=int, default=20)
+    ap.add_argument("--kernel-variant", type=int, default=0,
+                    help="usv_gmres_params.kernel_variant bits (0: the default kernel forms)")
     ap.add_argument("--capture", choices=("cycle", "stencil"), default=None,
                     help="run a short self-terminating workload for a profiler capture "
                          "(no bench line): `cycle` = --cycles restart cycles without CUDA "
@@ -250,6 +252,7 @@ def run_ours(args):
     it = solver.iterative_solver
     it.rtol, it.maxiter = args.rtol, args.maxiter
     it.backward_error_tol = 1e-4
+    it.kernel_variant = args.kernel_variant
     stream = torch.cuda.current_stream()
 
     def configure(precision, profile=False, its=None):
@@ -325,11 +328,12 @@ def run_ours(args):
                                         if v["ms"] > 0 and v["bytes"] > 0 else None}
                                     for k, v in prof_tot.items()}}
 
-    # the stencil alone: usv_operator_apply of the complex64 K rows and of the
-    # FP64 A rows on the batch, each launch timed with CUDA events after an L2
-    # flush; algorithmic bytes per launch: the per-node operator data once
-    # (complex64 row coefficients 48 B; FP64 diagonal + six edge coefficients
-    # 112 B) plus x and y of every RHS
+    # the stencil alone: usv_operator_apply_kernel of the complex64 K rows (both
+    # kernels: precomputed row coefficients, 48 B per node; 16-byte node
+    # records with the rows formed in registers) and of the FP64 A rows on the
+    # batch, launches timed with CUDA events after an L2 flush; algorithmic
+    # bytes per launch: the per-node operator data the kernel reads once plus x
+    # and y of every RHS
     if not args.no_stencil:
         from ultrasound_solver_b200 import _native as N
         op = solver.operator
@@ -338,16 +342,16 @@ def run_ours(args):
 
         import ctypes
 
-        def time_apply(x, variant, precision, reps=20):
+        def time_apply(x, variant, precision, kernel=N.STENCIL_AUTO, reps=20):
             # back-to-back launches through the C-ABI (the batch's operator data
-            # and vectors, >= 234 MB, exceed the 126 MB L2), after an L2 flush
+            # and vectors exceed the 126 MB L2), after an L2 flush
             y = torch.empty_like(x)
             lib, sh = N.load(), N.stream_handle(torch, x.device)
 
             def launch():
-                N.check(lib.usv_operator_apply(ctypes.byref(op.scene), N.ptr(op.buffer), variant,
-                                               precision, N.ptr(x), N.ptr(y), x.shape[0], op.n,
-                                               sh), "apply")
+                N.check(lib.usv_operator_apply_kernel(ctypes.byref(op.scene), N.ptr(op.buffer),
+                                                      variant, precision, kernel, N.ptr(x), N.ptr(y),
+                                                      x.shape[0], op.n, sh), "apply")
             for _ in range(3):
                 launch()
             flush.fill_(1)
@@ -361,20 +365,34 @@ def run_ours(args):
             return max_over_ranks(e0.elapsed_time(e1) / reps, world)
 
         x64 = rhs.to(torch.complex64).contiguous()
-        ms_k = time_apply(x64, N.APPLY_K, N.PREC_MIXED)
-        bytes_k = nn * (48.0 + args.batch * 16.0)
+        peak, peak_kind = measured_peak()
+        compulsory = nn * (16.0 + args.batch * 16.0)
+        kernels = {"k_apply_kc_rhs (complex64 row coefficients, 48 B per node)":
+                   (N.STENCIL_COEF_ROWS, nn * (48.0 + args.batch * 16.0))}
+        if args.batch <= 4:
+            kernels["k_apply_rec25 (16-byte node records, z-marching tiles)"] = (
+                N.STENCIL_RECORD_TILES, nn * (16.0 + args.batch * 16.0))
+        variants = {}
+        for name, (kern, nbytes) in kernels.items():
+            ms_k = time_apply(x64, N.APPLY_K, N.PREC_MIXED, kern)
+            variants[name] = {"us_per_launch": 1000.0 * ms_k, "bytes_per_launch": nbytes,
+                              "achieved": nbytes / (ms_k / 1e3) / 1e9,
+                              "frac": nbytes / (ms_k / 1e3) / 1e9 / peak,
+                              "compulsory_frac": compulsory / (ms_k / 1e3) / 1e9 / peak}
+        best = min(variants, key=lambda k: variants[k]["us_per_launch"])
         ms_a = time_apply(rhs.contiguous(), N.APPLY_A, N.PREC_FP64)
         bytes_a = nn * (112.0 + args.batch * 32.0)
-        peak, peak_kind = measured_peak()
+        b = variants[best]
         out["stencil"] = {
-            "kernel": f"k_apply_kc_rhs (complex64 K rows), {args.batch} RHS per launch",
-            "achieved": bytes_k / (ms_k / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
-            "frac": bytes_k / (ms_k / 1e3) / 1e9 / peak, "us_per_launch": 1000.0 * ms_k,
-            "bytes_per_launch": bytes_k, "l2": "inputs larger than L2 (20 launches back to back)",
-            # compulsory traffic of a minimal representation (3 real face
-            # coefficients + k^2 per node, fp32) against the same time
-            "compulsory_bytes_per_launch": nn * (16.0 + args.batch * 16.0),
-            "compulsory_frac": nn * (16.0 + args.batch * 16.0) / (ms_k / 1e3) / 1e9 / peak,
+            "kernel": f"{best}, {args.batch} RHS per launch",
+            "achieved": b["achieved"], "unit": "GB/s", "peak": peak, "peak_source": peak_kind,
+            "frac": b["frac"], "us_per_launch": b["us_per_launch"],
+            "bytes_per_launch": b["bytes_per_launch"],
+            "l2": "inputs larger than L2 (20 launches back to back)",
+            # compulsory traffic of a 16-byte-per-node operator record plus x
+            # and y of every RHS, against the same time
+            "compulsory_bytes_per_launch": compulsory, "compulsory_frac": b["compulsory_frac"],
+            "kernels": variants,
             "fp64_A": {"kernel": f"k_apply_fp64 (complex128 A rows), {args.batch} RHS per launch",
                        "achieved": bytes_a / (ms_a / 1e3) / 1e9,
                        "frac": bytes_a / (ms_a / 1e3) / 1e9 / peak,
@@ -643,6 +661,7 @@ def run_capture(args):
         it = solver.iterative_solver
         it.precision, it.restart = args.precision, args.restart
         it.recycle, it.recycle_every = args.recycle, args.recycle_every
+        it.kernel_variant = args.kernel_variant
         plain = min(args.cycles, 2) if args.recycle else args.cycles
         it.maxiter = plain * args.restart + (args.cycles - plain) * (args.restart - args.recycle)
         it.rtol, it.use_graph = 1e-12, False

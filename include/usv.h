@@ -135,8 +135,18 @@ typedef struct usv_gmres_params {
     int32_t max_ctas;            /* cap on the CTAs per right-hand side of the
                                     streaming kernels (each CTA then loops over
                                     more node chunks); 0 = fill the GPU          */
-    int32_t reserved;
+    int32_t kernel_variant;      /* USV_GMRES_* bits; 0 = the measured-fastest
+                                    forms (bulk-copy orthogonalisation ring,
+                                    per-warp dot tasks)                          */
 } usv_gmres_params;
+
+/* kernel_variant bits of usv_gmres_params (complex64 / bfloat16 vectors; the
+ * complex128 path always uses the per-thread / per-warp forms) */
+#define USV_GMRES_ORTH_CPASYNC 1   /* orthogonalisation: per-thread cp.async
+                                      pipeline instead of the bulk-copy ring  */
+#define USV_GMRES_DOTS_BULK 2      /* stencil + dots: bulk-copy tile ring with
+                                      per-warp node slices instead of per-warp
+                                      dot tasks with direct loads              */
 
 typedef struct usv_gmres_stats {
     int32_t status;              /* USV_OK or USV_ERR_*                          */
@@ -180,6 +190,19 @@ int usv_operator_build(const usv_scene* scene, const double* rho, const double* 
 int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant,
                        int precision, const void* x, void* y, int nrhs, int64_t ld,
                        void* stream);
+/* usv_operator_apply with an explicit stencil kernel for USV_APPLY_K / KH in
+ * complex64 (USV_PREC_MIXED); other variants and precisions ignore `kernel`.
+ * Replaces the same SpMV as usv_operator_apply; the kernel choice is what
+ * autotune.StencilTuner measures. */
+#define USV_STENCIL_AUTO 0          /* the library's default for the batch     */
+#define USV_STENCIL_COEF_ROWS 1     /* precomputed complex64 row coefficients
+                                       (48 B per node), one thread per node    */
+#define USV_STENCIL_RECORD_TILES 2  /* 16-B node records {rho, R, s}, rows
+                                       formed in registers, z-marching tiles;
+                                       nrhs <= 4                               */
+int usv_operator_apply_kernel(const usv_scene* scene, const void* op_buf, int variant,
+                              int precision, int kernel, const void* x, void* y, int nrhs,
+                              int64_t ld, void* stream);
 /* Copies of the per-node diagonal (complex128), row scale R and Jacobi s
  * (forward, adjoint) for inspection; any pointer may be NULL. */
 int usv_operator_export(const usv_scene* scene, const void* op_buf, double* diag,
@@ -196,6 +219,24 @@ int usv_gmres_solve(const usv_scene* scene, const void* op_buf,
                     const usv_gmres_params* params, const void* rhs, void* x,
                     int nrhs, int64_t ld, void* workspace, size_t workspace_bytes,
                     usv_gmres_stats* stats, void* stream);
+
+/* Several scenes in one batched solve (the uneven-grid scene batches): the
+ * right-hand side b belongs to scene scene_of_rhs[b] < nscenes, whose
+ * operator buffer is op_bufs[scene]. Every kernel launch of a restart cycle
+ * covers all right-hand sides of all scenes. rhs and x are columns of stride
+ * ld >= the largest scene's node count; a right-hand side of a smaller scene
+ * uses the first n entries of its column. All scenes share the parameters
+ * (restart, recycling, precision, adjoint); the restart length must not be
+ * cut by a scene smaller than it. Replaces the per-scene loop over
+ * HelmholtzDirectSolver solves (phase_response_basis.py:97-115 batches one
+ * scene's columns; scenes were solved one after the other). */
+int usv_gmres_scenes_workspace_bytes(int nscenes, const usv_scene* scenes,
+                                     const int* scene_of_rhs, const usv_gmres_params* params,
+                                     int nrhs, size_t* bytes);
+int usv_gmres_solve_scenes(int nscenes, const usv_scene* scenes, const void* const* op_bufs,
+                           const int* scene_of_rhs, const usv_gmres_params* params,
+                           const void* rhs, void* x, int nrhs, int64_t ld, void* workspace,
+                           size_t workspace_bytes, usv_gmres_stats* stats, void* stream);
 
 /* ---- scene set-up ------------------------------------------------------ */
 /* rho, c from an SDF: h = sine-smoothed step over +-width, blend 1/rho and

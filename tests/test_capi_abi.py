@@ -114,3 +114,34 @@ def test_harmonic_ritz_matches_scipy(lib, m, k, aug):
         assert np.linalg.norm(M1 @ P[:, i] - th[i] * (M2 @ P[:, i])) <= 1e-10 * np.linalg.norm(M1)
     assert lib.usv_harmonic_ritz(m, m + 1, Gf.ctypes.data, Wf.ctypes.data, P.ctypes.data,
                                  th.ctypes.data) == 1
+
+
+def test_scene_batch_workspace_and_argument_checks(lib):
+    """usv_gmres_scenes_workspace_bytes (host only): the workspace covers the
+    largest scene; a scene index out of range, or a scene with fewer nodes
+    than the restart length (which would cut every scene's cycle), is refused."""
+    def scene(n):
+        s = _native.Scene()
+        s.nx = s.ny = s.nz = n
+        s.dx, s.omega, s.pml_order = 1e-3, 2.5e5, 3
+        return s
+    scenes = (_native.Scene * 2)(scene(9), scene(12))
+    p = _native.GmresParams()
+    p.restart, p.maxiter, p.rtol, p.backward_error_tol = 30, 100, 1e-6, 1e-4
+    p.precision, p.history_capacity = _native.PREC_MIXED, 4
+    owner = (ctypes.c_int * 3)(0, 1, 1)
+    nbytes = ctypes.c_size_t()
+    assert lib.usv_gmres_scenes_workspace_bytes(2, scenes, owner, ctypes.byref(p), 3,
+                                                ctypes.byref(nbytes)) == _native.USV_OK
+    one = (_native.Scene * 1)(scene(12))
+    same = (ctypes.c_int * 3)(0, 0, 0)
+    big = ctypes.c_size_t()
+    assert lib.usv_gmres_scenes_workspace_bytes(1, one, same, ctypes.byref(p), 3,
+                                                ctypes.byref(big)) == _native.USV_OK
+    assert nbytes.value == big.value  # laid out for the largest scene
+    bad = (ctypes.c_int * 3)(0, 2, 1)
+    assert lib.usv_gmres_scenes_workspace_bytes(2, scenes, bad, ctypes.byref(p), 3,
+                                                ctypes.byref(nbytes)) == _native.USV_ERR_ARG
+    tiny = (_native.Scene * 2)(scene(3), scene(12))  # 27 nodes < restart 30
+    assert lib.usv_gmres_scenes_workspace_bytes(2, tiny, owner, ctypes.byref(p), 3,
+                                                ctypes.byref(nbytes)) == _native.USV_ERR_ARG

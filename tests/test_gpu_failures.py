@@ -87,7 +87,7 @@ def test_lucky_breakdown_ends_cleanly(n, precision, recycle):
         M = A.conj().T if adjoint else A
         for k in range(2):
             want = np.linalg.solve(M, b[k])
-            assert rel(x[k], want) <= 1e-9
+            assert rel(x[k], want) <= (1e-9 if precision == "fp64" else 1e-8)
             assert it.last_stats[k]["status"] == N.USV_OK
         if precision == "fp64":  # exact breakdown: the first cycle ends it
             assert it.last_iterations <= 2 * it.restart

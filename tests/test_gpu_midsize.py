@@ -110,3 +110,20 @@ def test_fp64_iterations_independent_of_cta_cap(mid):
         s.solve()
         counts.append(s.iterative_solver.last_iterations)
     assert max(counts) - min(counts) <= 30, counts
+
+
+@pytest.mark.parametrize("precision", ["mixed", "bf16"])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_arnoldi_kernel_variants(mid, precision, variant):
+    """Every form of the Arnoldi kernels (default: bulk-copy orthogonalisation
+    ring and per-warp dot tasks; the per-thread cp.async orthogonalisation;
+    the bulk-copy dot ring; both) gives the reference's solutions on the
+    capped grid, plain and recycled."""
+    for algorithm in ("gmres30", "gcrodr36_8"):
+        s = _solver(mid, precision, algorithm)
+        s.iterative_solver.kernel_variant = variant
+        cols = s.sources.column_rhs(s.transducers.amplitudes)[:3]
+        x = s.solve_rhs_device(cols).cpu().numpy()
+        G = mid["G"].astype(np.complex128)
+        for k in range(3):
+            assert rel(x[k], G[:, k]) <= TOL, (algorithm, k)

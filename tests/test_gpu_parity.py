@@ -56,17 +56,23 @@ def test_scaled_jacobi_operator(golden):
         np.testing.assert_allclose((jaca if adj else jac).cpu().numpy(), inv_d, rtol=1e-12)
 
 
+@pytest.mark.parametrize("kernel", ["coef_rows", "record_tiles"])
 @pytest.mark.parametrize("nrhs", [1, 2, 3, 4, 5, 8, 11])
-def test_mixed_apply_batches(golden, nrhs):
-    """Complex64 K / K^H on a batch (one-, two- and per-node-loop kernels by batch
-    size) against the FP64 rows of every column."""
+def test_mixed_apply_batches(golden, nrhs, kernel):
+    """Complex64 K / K^H on a batch (coefficient rows: one-, two- and
+    per-node-loop kernels by batch size; record tiles: z-marching kernel from
+    the 16-byte node records, up to 4 right-hand sides) against the FP64 rows
+    of every column."""
     from ultrasound_solver_b200 import _native as N
+    k = {"coef_rows": N.STENCIL_COEF_ROWS, "record_tiles": N.STENCIL_RECORD_TILES}[kernel]
+    if k == N.STENCIL_RECORD_TILES and nrhs > 4:
+        pytest.skip("the record-tile kernel takes at most 4 right-hand sides")
     s = golden_solver(golden)
     rng = np.random.default_rng(nrhs)
     x = rng.standard_normal((nrhs, s.operator.n)) + 1j * rng.standard_normal((nrhs, s.operator.n))
     xt = torch.from_numpy(x).cuda()
     for var in (N.APPLY_K, N.APPLY_KH):
-        got = s.operator.apply(xt.to(torch.complex64), var, N.PREC_MIXED).cpu().numpy()
+        got = s.operator.apply(xt.to(torch.complex64), var, N.PREC_MIXED, kernel=k).cpu().numpy()
         want = s.operator.apply(xt, var, N.PREC_FP64).cpu().numpy()
         for b in range(nrhs):
             assert rel(got[b], want[b]) < 2e-6

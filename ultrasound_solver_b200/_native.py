@@ -28,6 +28,8 @@ USV_ERR_DEVICE_TIMEOUT = 10
 FACE_REFLECTING, FACE_OPEN, FACE_SOFT, FACE_IMPEDANCE = 0, 1, 2, 3
 APPLY_A, APPLY_AH, APPLY_ABS_A, APPLY_ABS_AH, APPLY_K, APPLY_KH = range(6)
 PREC_FP64, PREC_MIXED, PREC_MIXED_BF16 = 0, 1, 2
+GMRES_ORTH_CPASYNC, GMRES_DOTS_BULK = 1, 2
+STENCIL_AUTO, STENCIL_COEF_ROWS, STENCIL_RECORD_TILES = 0, 1, 2
 LOSS_FOCAL_PRESSURE, LOSS_FOCAL_CONTRAST, LOSS_CONTRAST_RATIO = 0, 1, 2
 
 
@@ -59,7 +61,7 @@ class GmresParams(C.Structure):
                 ("history", C.POINTER(C.c_double)),
                 ("profile", C.POINTER(GmresProfile)),
                 ("recycle", C.c_int32), ("recycle_every", C.c_int32),
-                ("max_ctas", C.c_int32), ("reserved", C.c_int32)]
+                ("max_ctas", C.c_int32), ("kernel_variant", C.c_int32)]
 
 
 class GmresStats(C.Structure):
@@ -84,10 +86,15 @@ _SIGNATURES = {
     "usv_operator_bytes": ([_SP, C.POINTER(_SZ)], _I),
     "usv_operator_build": ([_SP, _P, _P, _P, _SZ, _P], _I),
     "usv_operator_apply": ([_SP, _P, _I, _I, _P, _P, _I, _I64, _P], _I),
+    "usv_operator_apply_kernel": ([_SP, _P, _I, _I, _I, _P, _P, _I, _I64, _P], _I),
     "usv_operator_export": ([_SP, _P, _P, _P, _P, _P, _P, _P], _I),
     "usv_gmres_workspace_bytes": ([_SP, C.POINTER(GmresParams), _I, C.POINTER(_SZ)], _I),
     "usv_gmres_solve": ([_SP, _P, C.POINTER(GmresParams), _P, _P, _I, _I64, _P, _SZ,
                          C.POINTER(GmresStats), _P], _I),
+    "usv_gmres_scenes_workspace_bytes": ([_I, _SP, _P, C.POINTER(GmresParams), _I,
+                                          C.POINTER(_SZ)], _I),
+    "usv_gmres_solve_scenes": ([_I, _SP, _P, _P, C.POINTER(GmresParams), _P, _P, _I, _I64, _P,
+                                _SZ, C.POINTER(GmresStats), _P], _I),
     "usv_materials_blend": ([_SP, _P, _P, _D, _D, _D, _D, _P, _P, _D, _D, _P, _P, _P], _I),
     "usv_source_masses": ([_SP, _P, _P, _P, _I, _D, _P, _P, _P, _I, _P, _P], _I),
     "usv_source_rhs": ([_SP, _P, _I, _P, _D, _P, _I, _I64, _P], _I),

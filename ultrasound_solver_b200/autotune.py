@@ -1,4 +1,4 @@
-"""Batch-width autotuner for the batched GMRES launches.
+"""Autotuners for the batched GMRES launches and the stencil kernels.
 
 How many right-hand sides go through one usv_gmres_solve launch decides how
 well the persistent grids fill the GPU (few RHS: per-launch latency and the
@@ -6,9 +6,13 @@ per-cycle host round trip dominate; many: the Krylov workspace grows as
 B (m+1) N and each RHS gets fewer CTAs). BatchTuner times a few restart
 cycles of the real operator at each candidate width that fits the memory
 budget and keeps the width with the lowest time per right-hand-side
-iteration. Results are cached in a JSON file keyed by
-(GPU name, grid, precision, restart, recycle, adjoint), so the measurement
-runs once per machine and scene shape.
+iteration; it then times the Arnoldi kernel forms at that width (the
+default, the per-thread cp.async orthogonalisation, the bulk-copy dot ring:
+usv_gmres_params.kernel_variant) and keeps the fastest. StencilTuner picks the complex64 operator-apply
+kernel (precomputed row coefficients, one thread per node, or 16-byte node
+records with z-marching tiles) for a grid and batch width. Results are cached
+in a JSON file keyed by GPU name, grid and the solver settings, so each
+measurement runs once per machine and scene shape.
 """
 from __future__ import annotations
 
@@ -77,6 +81,7 @@ class BatchTuner:
                         adjoint)
         if not force and key in self.cache:
             solver.batch_width = int(self.cache[key]["batch_width"])
+            solver.kernel_variant = int(self.cache[key].get("kernel_variant", 0))
             return solver.batch_width
         saved = (solver.maxiter, solver.rtol, solver.batch_width, solver.profile)
         steps = max(solver.restart - max(solver.recycle, 0), 1)
@@ -98,8 +103,81 @@ class BatchTuner:
             solver.maxiter, solver.rtol, solver.batch_width, solver.profile = saved
         best = min(timings, key=timings.get)
         self.last_timings = timings
+        variant, variant_timings = self._tune_variant(solver, operator, rhs, best, adjoint)
         self.cache[key] = {"batch_width": best,
-                           "seconds_per_rhs_iteration": {str(k): v for k, v in timings.items()}}
+                           "seconds_per_rhs_iteration": {str(k): v for k, v in timings.items()},
+                           "kernel_variant": variant,
+                           "seconds_per_rhs_iteration_by_variant": variant_timings}
         self._save()
         solver.batch_width = best
+        solver.kernel_variant = variant
+        return best
+
+    def _tune_variant(self, solver, operator, rhs, width, adjoint):
+        """Time the Arnoldi kernel forms at `width` (complex64 / bfloat16 only)."""
+        if solver.precision in ("fp64", "complex128"):
+            return solver.kernel_variant, {}
+        from . import _native as N
+        saved = (solver.maxiter, solver.rtol, solver.batch_width, solver.profile,
+                 solver.kernel_variant)
+        steps = max(solver.restart - max(solver.recycle, 0), 1)
+        solver.maxiter = self.cycles * solver.restart + (3 if solver.recycle else 1) * steps
+        solver.rtol, solver.batch_width, solver.profile = 0.0, 0, False
+        idx = torch.arange(width, device=rhs.device) % rhs.shape[0]
+        batch = rhs[idx]
+        timings = {}
+        try:
+            for variant in (0, N.GMRES_ORTH_CPASYNC, N.GMRES_DOTS_BULK):
+                solver.kernel_variant = variant
+                solver.solve(operator, batch, adjoint=adjoint, raise_on_failure=False)
+                torch.cuda.synchronize(operator.device)
+                t0 = time.perf_counter()
+                solver.solve(operator, batch, adjoint=adjoint, raise_on_failure=False)
+                torch.cuda.synchronize(operator.device)
+                timings[variant] = (time.perf_counter() - t0) / max(solver.last_iterations, 1) / width
+        finally:
+            (solver.maxiter, solver.rtol, solver.batch_width, solver.profile,
+             solver.kernel_variant) = saved
+        return min(timings, key=timings.get), {str(k): v for k, v in timings.items()}
+
+
+class StencilTuner:
+    """Pick the complex64 K / K^H apply kernel for one operator and batch width."""
+
+    def __init__(self, cache_path: str | Path | None = None, reps: int = 10):
+        self.cache_path = Path(cache_path) if cache_path else DEFAULT_CACHE
+        self.reps = int(reps)
+        self.last_timings = {}
+
+    def tune(self, operator, nrhs: int, adjoint: bool = False, force: bool = False) -> int:
+        """Measure (or read from the cache) the faster kernel; sets operator.stencil_kernel."""
+        from . import _native as N
+        name = torch.cuda.get_device_name(operator.device)
+        grid = "x".join(str(int(v)) for v in operator.shape)
+        key = f"stencil|{name}|{grid}|b{int(nrhs)}|{'adj' if adjoint else 'fwd'}"
+        cache = BatchTuner(self.cache_path).cache
+        if not force and key in cache:
+            operator.stencil_kernel = int(cache[key]["kernel"])
+            return operator.stencil_kernel
+        variant = N.APPLY_KH if adjoint else N.APPLY_K
+        x = torch.randn((int(nrhs), operator.n), dtype=torch.complex64, device=operator.device)
+        candidates = [N.STENCIL_COEF_ROWS] + ([N.STENCIL_RECORD_TILES] if nrhs <= 4 else [])
+        timings = {}
+        for k in candidates:
+            for _ in range(2):
+                operator.apply(x, variant, N.PREC_MIXED, kernel=k)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(self.reps):
+                operator.apply(x, variant, N.PREC_MIXED, kernel=k)
+            e1.record()
+            torch.cuda.synchronize(operator.device)
+            timings[k] = e0.elapsed_time(e1) / self.reps
+        best = min(timings, key=timings.get)
+        self.last_timings = timings
+        tuner = BatchTuner(self.cache_path)
+        tuner.cache[key] = {"kernel": best, "ms_per_apply": {str(k): v for k, v in timings.items()}}
+        tuner._save()
+        operator.stencil_kernel = best
         return best

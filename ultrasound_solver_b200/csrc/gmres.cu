@@ -99,7 +99,28 @@ struct GState {
     double2* alpha;    // [B][k] projection C^H r of the cycle's first residual
     int* klast;        // [B] recycled count of the last finished cycle
     int* started;      // [B]
+    const struct SceneSlot* slots;  // [B] multi-scene solves: the scene of each RHS
 };
+
+// Scene of one right-hand side of a multi-scene solve (usv_gmres_solve_scenes):
+// the operator views, node count and chunk count of that scene and the node
+// steps of the 256- and kDotsThreads-thread kernels. Kernels instantiated
+// with MS = true read their scene from here (blockIdx.y = right-hand side);
+// single-scene kernels take it from their arguments.
+struct SceneSlot {
+    OpView<double> op64;
+    OpView<float> op32;
+    long long n;
+    int nchunk;
+    Step step, step_d;
+};
+template <typename R> __device__ __forceinline__ const OpView<R>& slot_view(const SceneSlot& s);
+template <> __device__ __forceinline__ const OpView<double>& slot_view<double>(const SceneSlot& s) {
+    return s.op64;
+}
+template <> __device__ __forceinline__ const OpView<float>& slot_view<float>(const SceneSlot& s) {
+    return s.op32;
+}
 
 // host-read block offsets (in doubles)
 __host__ __device__ __forceinline__ int hb_graw(int) { return 0; }
@@ -113,6 +134,7 @@ struct WsLayout {
     size_t V, partial, H, gc, gs, g, y, sigma, bnorm, atol, wnorm, gates, hist, status, cycles,
         iters, len, ended, counter, state_begin, total;
     size_t U, C, bpart, coef, hb, dU, alpha, klast, started, ctl;  // recycling
+    size_t slots;  // multi-scene solves: SceneSlot per right-hand side
 };
 
 static long long padded(long long n) { return (n + 63) / 64 * 64; }
@@ -163,6 +185,7 @@ static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes,
         L.klast = take(sizeof(int) * B);
         L.started = take(sizeof(int) * B);
     }
+    L.slots = take(sizeof(SceneSlot) * size_t(B));
     L.total = off;
     return L;
 }
@@ -223,20 +246,27 @@ __device__ __forceinline__ CycleBasis<S> cycle_basis(S* V, const GState& g, int 
 // r = Rs rhs. Recycled cycles (kc > 0) also set up the fixed leading block of
 // G = [[D, B], [0, Hbar]]: columns t < kc are d_t e_t (identity rotations),
 // C slots have unit scale; the projection kernels then form beta.
-template <bool ADJ, typename C2>
+template <bool ADJ, typename C2, bool MS = false>
 __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const double2* rhs,
                                                   const double2* x, long long ld, C2* V,
                                                   GState g, int first, Step step) {
     const int b = blockIdx.y;
     if (g.kr > 0) first = !g.started[b];
     if (!first && (g.status[b] != ST_ACTIVE)) return;
+    int nchunk = g.nchunk;
+    if constexpr (MS) {
+        const SceneSlot& sl = g.slots[b];
+        op = sl.op64;
+        step = sl.step;
+        nchunk = sl.nchunk;
+    }
     __shared__ double sh[32];
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     C2* v0 = cb.V + (long long)cb.kc * g.nv;
     double acc = 0.0, acc_s = 0.0;
-    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * g.chunk;
         const long long n1 = min(n0 + g.chunk, op.n);
         Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
@@ -400,7 +430,7 @@ template <> struct MathT<bf2> {
     using T2 = float2;
 };
 __device__ __forceinline__ double2 to_d(double2 a);
-__device__ __forceinline__ float2 to_f(bf2 a) { return __bfloat1622float2(a); }
+__device__ __forceinline__ float2 to_f(bf2 a) { return bf2_to_f2(a); }
 
 // Complex value c (0/1) of pair k of stage t % S (in the pass arithmetic).
 template <typename C2>
@@ -560,6 +590,40 @@ template <> struct LaneLoad<double2> {
     __device__ __forceinline__ double2 get(int i) const { return i ? b : a; }
 };
 
+// Last CTA of a dots launch: sum the per-CTA partials of t = 0..j (the dots)
+// and t = j+1 (||w||^2) in a fixed order into Hessenberg column j (or the
+// projection coefficients alpha) and wnorm.
+__device__ __forceinline__ void dots_finish(GState& g, int b, int j, bool proj) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = int(blockDim.x >> 5);
+    const int nparts = int(gridDim.x);
+    for (int t = warp; t <= j + 1; t += nw) {
+        double re0 = 0.0, im0 = 0.0;
+        const double2* pt = g.partial + (long long)b * g.nblk * g.ps + t;
+        for (int q0 = 0; q0 < nparts; q0 += 32 * 4) {
+            double2 pv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + 32 * u + lane;
+                pv[u] = q < nparts ? ld_cg(pt + (long long)q * g.ps) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                re0 += pv[u].x;
+                im0 += pv[u].y;
+            }
+        }
+        re0 = warp_sum(re0);
+        im0 = warp_sum(im0);
+        if (lane == 0) {
+            if (t > j) g.wnorm[b] = sqrt(re0);
+            else if (proj) g.alpha[(long long)b * g.kr + t] = make_double2(re0, im0);
+            else g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
+        }
+    }
+    if (threadIdx.x == 0) g.counter[b] = 0;
+}
+
 // Arnoldi step j, part 1: each CTA computes its chunk of w = sigma_j K u_j
 // (stencil) into shared and global memory, then the dots <sigma_t u_t, w>,
 // t <= j, and ||w||^2. (A separate stencil kernel ahead of a streaming dots
@@ -570,12 +634,16 @@ template <> struct LaneLoad<double2> {
 // complex64.)
 // mode 1 (recycled cycles): no stencil; the dots alpha_t = <C_t, r> of the
 // cycle's first residual r (slot kc) with the recycled C_t, t < kc.
-template <typename R, typename S, bool ADJ, int NT>
+template <typename R, typename S, bool ADJ, int NT, bool MS = false>
 __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, int j, Step step,
                                                 int mode) {
     using C2 = S;  // stored vector element
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    if constexpr (MS) {
+        op = slot_view<R>(g.slots[b]);
+        step = g.slots[b].step_d;
+    }
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     const bool proj = mode == 1;
     if (proj) {
@@ -722,32 +790,218 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         part[t] = make_double2(re, im);
     }
     if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    const int nparts = int(gridDim.x);
-    for (int t = warp; t <= j + 1; t += nw) {
-        double re0 = 0.0, im0 = 0.0;
-        const double2* pt = g.partial + (long long)b * g.nblk * g.ps + t;
-        for (int q0 = 0; q0 < nparts; q0 += 32 * 4) {
-            double2 pv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int q = q0 + 32 * u + lane;
-                pv[u] = q < nparts ? ld_cg(pt + (long long)q * g.ps) : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                re0 += pv[u].x;
-                im0 += pv[u].y;
-            }
+    dots_finish(g, b, j, proj);
+}
+
+// Bulk-copy form of k_dots (bfloat16 and complex64 vectors). Per chunk of DC
+// nodes the consumer warps first form w = sigma_j K u_j (stencil, into shared
+// memory and the basis) while a producer warp already streams the chunk tiles
+// of u_0 .. u_j into a ring of shared-memory stages (cp.async.bulk completed
+// on full / empty mbarriers, kDotsStages - 1 tiles ahead). Every consumer
+// warp then owns one 1/16 slice of the chunk and forms its partial
+// <sigma_t u_t, w> for every tile t, reduced over the warp and added in FP64
+// to its own row of per-warp sums (no load imbalance between the dot tasks);
+// ||w||^2 is summed while w is formed. All waits are bounded
+// (ST_DEVICE_TIMEOUT, then a bounded drain of the copies in flight).
+template <typename S> struct DotsBulk {
+    static constexpr int DC = std::is_same<S, bf2>::value ? 2 * kChunk : kChunk;  // nodes per chunk
+    static constexpr int TILE = DC * int(sizeof(S));
+    static constexpr int STAGES = 4;
+    static constexpr int NWC = kDotsThreads / 32;                                // consumer warps
+    using YS = typename std::conditional<std::is_same<S, float2>::value, double2, S>::type;
+    static constexpr int THREADS = kDotsThreads + 32;
+    // ring, w of the chunk, per-warp sums of the m + 1 dots, barriers
+    static size_t smem(int m) {
+        return size_t(STAGES) * TILE + size_t(DC) * sizeof(YS) +
+               size_t(NWC) * size_t(m + 1) * sizeof(double2) + 2 * STAGES * sizeof(unsigned long long);
+    }
+};
+
+template <typename R, typename S, bool ADJ, bool MS = false>
+__global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R> op, S* V, GState g,
+                                                                      int j, Step step, int mode) {
+    using C2 = S;
+    using P = DotsBulk<S>;
+    using YS = typename P::YS;
+    constexpr int DC = P::DC, NWC = P::NWC;
+    constexpr int NL = LaneLoad<C2>::NL;        // nodes per 16-byte group
+    constexpr int GPW = DC / NL / NWC / 32;     // groups per lane and tile
+    static_assert(GPW >= 1 && DC % (NL * NWC * 32) == 0, "chunk / warp slicing");
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    if constexpr (MS) {
+        op = slot_view<R>(g.slots[b]);
+        step = g.slots[b].step_d;
+    }
+    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    const bool proj = mode == 1;
+    if (proj) {
+        if (cb.kc == 0) return;
+        j = cb.kc - 1;
+    } else if (j < cb.kc) {
+        return;
+    }
+    extern __shared__ __align__(128) char dyn[];
+    char* ring = dyn;
+    YS* ys = reinterpret_cast<YS*>(dyn + size_t(P::STAGES) * P::TILE);
+    const int wst = g.m + 1;  // row stride of the per-warp sums
+    double2* wsum = reinterpret_cast<double2*>(reinterpret_cast<char*>(ys) + size_t(DC) * sizeof(YS));
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(
+        reinterpret_cast<char*>(wsum) + size_t(NWC) * wst * sizeof(double2));
+    unsigned long long* empty = full + P::STAGES;
+    __shared__ double sh[32];
+    __shared__ int failed;
+    const long long N = op.n;
+    const C2* uj = cb.V + (long long)j * g.nv;
+    C2* w = cb.V + (long long)(j + 1) * g.nv;
+    const R sj = R(g.sigma[b * (g.m + 1) + j]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < NWC * wst; i += blockDim.x) wsum[i] = make_double2(0.0, 0.0);
+    if (threadIdx.x == 0) {
+        failed = 0;
+        for (int st = 0; st < P::STAGES; ++st) {
+            mbar_init(&full[st], 1);
+            mbar_init(&empty[st], NWC);
         }
-        re0 = warp_sum(re0);
-        im0 = warp_sum(im0);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const int nphase = int((N + DC - 1) / DC);
+    const int nmy = nphase > int(blockIdx.x) ? (nphase - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x) : 0;
+    const int tpc = j + 1;  // tiles per chunk: u_0 .. u_j
+    double wn = 0.0;        // ||w||^2 of this thread's nodes
+    if (warp == NWC) {
+        // producer warp: one elected thread issues the tiles of every chunk
         if (lane == 0) {
-            if (t > j) g.wnorm[b] = sqrt(re0);
-            else if (proj) g.alpha[(long long)b * g.kr + t] = make_double2(re0, im0);
-            else g.H[((long long)b * g.m + j) * (g.m + 1) + t] = make_double2(re0, im0);
+            long long q = 0;
+            bool ok = true;
+            for (int i = 0; i < nmy && ok; ++i) {
+                const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * DC;
+                const int len = int(min((long long)DC, N - n0));
+                const unsigned bytes = unsigned((size_t(len) * sizeof(C2) + 15) / 16 * 16);
+                for (int t = 0; t < tpc; ++t, ++q) {
+                    const int st = int(q % P::STAGES);
+                    if (!mbar_wait(&empty[st], unsigned((q / P::STAGES) & 1) ^ 1u)) {
+                        ok = false;
+                        break;
+                    }
+                    const C2* src = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
+                    mbar_expect_tx(&full[st], bytes);
+                    bulk_g2s(ring + size_t(st) * P::TILE, src, bytes, &full[st]);
+                }
+            }
+            if (!ok) {
+                failed = 1;
+                g.status[b] = ST_DEVICE_TIMEOUT;
+            }
+            for (long long r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
+                mbar_wait(&full[r % P::STAGES], unsigned((r / P::STAGES) & 1));
+        }
+    } else {
+        long long q = 0;
+        for (int i = 0; i < nmy; ++i) {
+            const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * DC;
+            const int len = int(min((long long)DC, N - n0));
+            // all consumer warps are done with ys of the previous chunk; a
+            // failed wait of any warp (seen by all after the barrier) ends
+            // the loop for every consumer at the same point
+            asm volatile("bar.sync 1, %0;" ::"n"(kDotsThreads) : "memory");
+            if (failed) break;
+            if (mode == 0) {
+                Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
+                constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
+#pragma unroll(kStencilUnroll)
+                for (int e = threadIdx.x; e < DC; e += kDotsThreads) {
+                    C2 y = from_d<C2>(make_double2(0.0, 0.0));
+                    if (e < len) {
+                        const long long n = n0 + e;
+                        y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
+                        w[n] = y;
+                        wn += double(cabs2(to_d(y)));
+                    }
+                    ys[e] = as_ys<YS>(y);
+                    advance(p, step, op.nx, op.ny);
+                }
+            } else {
+                for (int e = threadIdx.x; e < DC; e += kDotsThreads) {
+                    const C2 y = e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0));
+                    wn += double(cabs2(to_d(y)));
+                    ys[e] = as_ys<YS>(y);
+                }
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(kDotsThreads) : "memory");
+            const int nvalid = (len + NL - 1) / NL;  // groups holding a node of the chunk
+            bool ok = true;
+            for (int t = 0; t < tpc; ++t, ++q) {
+                const int st = int(q % P::STAGES);
+                if (!mbar_wait(&full[st], unsigned((q / P::STAGES) & 1))) {
+                    ok = false;
+                    break;
+                }
+                const char* tile = ring + size_t(st) * P::TILE;
+                float fre = 0.f, fim = 0.f;
+                double dre = 0.0, dim = 0.0;
+#pragma unroll
+                for (int u = 0; u < GPW; ++u) {
+                    const int qg = (warp * GPW + u) * 32 + lane;  // 16-byte group of the tile
+                    if (qg >= nvalid) continue;
+                    if constexpr (std::is_same<C2, bf2>::value) {
+                        const uint4 a = reinterpret_cast<const uint4*>(tile)[qg];
+                        const uint4 y = reinterpret_cast<const uint4*>(ys)[qg];
+                        float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
+                        bf_mac(rr, ii, ri, ir, a.x, y.x);
+                        bf_mac(rr, ii, ri, ir, a.y, y.y);
+                        bf_mac(rr, ii, ri, ir, a.z, y.z);
+                        bf_mac(rr, ii, ri, ir, a.w, y.w);
+                        fre += rr + ii;
+                        fim += ri - ir;
+                    } else {
+                        const float4 a = reinterpret_cast<const float4*>(tile)[qg];
+                        const double2 y0 = ys[2 * qg], y1 = ys[2 * qg + 1];
+                        dre = fma(double(a.x), y0.x, fma(double(a.y), y0.y, dre));
+                        dim = fma(double(a.x), y0.y, fma(-double(a.y), y0.x, dim));
+                        dre = fma(double(a.z), y1.x, fma(double(a.w), y1.y, dre));
+                        dim = fma(double(a.z), y1.y, fma(-double(a.w), y1.x, dim));
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[st]);
+                double re, im;
+                if constexpr (std::is_same<C2, bf2>::value) {
+                    re = double(fre);
+                    im = double(fim);
+                } else {
+                    re = dre;
+                    im = dim;
+                }
+                re = warp_sum(re);
+                im = warp_sum(im);
+                if (lane == 0) {
+                    double2& acc = wsum[warp * wst + t];
+                    acc = make_double2(acc.x + re, acc.y + im);
+                }
+            }
+            if (!ok) {
+                failed = 1;
+                g.status[b] = ST_DEVICE_TIMEOUT;
+            }
         }
     }
-    if (threadIdx.x == 0) g.counter[b] = 0;
+    wn = block_sum(wn, sh);
+    if (failed) return;
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+    for (int t = threadIdx.x; t <= j; t += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int ww = 0; ww < NWC; ++ww) {
+            re += wsum[ww * wst + t].x;
+            im += wsum[ww * wst + t].y;
+        }
+        const double st = g.sigma[b * (g.m + 1) + t];
+        part[t] = make_double2(re * st, im * st);
+    }
+    if (threadIdx.x == 0) part[j + 1] = make_double2(wn, 0.0);
+    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    dots_finish(g, b, j, proj);
 }
 
 // d = a * b + c on two fp32 lanes at once (PTX fma.rn.f32x2, sm_100)
@@ -859,11 +1113,16 @@ __device__ __forceinline__ void orth_finish(GState& g, int b, const CycleBasis<C
 // ------------------------------------------------------------ Arnoldi: orthogonalise + norm
 // proj = 1 (recycled cycles): r -= sum_t alpha_t C_t on the cycle's first
 // residual (slot kc), then beta = ||r|| starts the Krylov part of the cycle.
-template <typename S>
+template <typename S, bool MS = false>
 __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, int j, int proj) {
     using C2 = S;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    int nchunk = g.nchunk;
+    if constexpr (MS) {
+        N = g.slots[b].n;
+        nchunk = g.slots[b].nchunk;
+    }
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     if (proj) {
         if (cb.kc == 0) return;
@@ -886,7 +1145,7 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     }
     __syncthreads();  // hs, hm visible
     double acc = 0.0;
-    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
         C2* w = cb.V + (long long)(j + 1) * g.nv + n0;
@@ -952,13 +1211,16 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
 // in flight, and the CTA leaves.
 template <typename S> struct OrthBulk {
     static constexpr int TILE = kChunk * int(sizeof(S));   // bytes per chunk tile
-    static constexpr int STAGES = sizeof(S) == 4 ? 6 : (sizeof(S) == 8 ? 4 : 3);
+    // stages: a power of two (ring index and phase by mask and shift)
+    static constexpr int LOG_STAGES = sizeof(S) == 4 ? 3 : 2;
+    static constexpr int STAGES = 1 << LOG_STAGES;
     static constexpr size_t SMEM = size_t(STAGES) * TILE + 2 * STAGES * sizeof(unsigned long long);
     static constexpr int THREADS = kThreads + 32;           // + the producer warp
 };
 
-// values of this thread's pairs from a chunk tile (nodes >= len read as zero)
-template <typename C2, typename M2>
+// values of this thread's pairs from a chunk tile (MASK: nodes >= len read as
+// zero; only the last, partial chunk of a vector needs it)
+template <typename C2, bool MASK, typename M2>
 __device__ __forceinline__ void tile_pairs(const char* tile, int len, M2 (&v)[kPairs][2]) {
     if constexpr (std::is_same<C2, bf2>::value) {
 #pragma unroll
@@ -968,35 +1230,41 @@ __device__ __forceinline__ void tile_pairs(const char* tile, int len, M2 (&v)[kP
             const unsigned w4[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                v[2 * u + c / 2][c % 2] = e + c < len ? to_f(*reinterpret_cast<const bf2*>(&w4[c]))
-                                                      : cmake<M2>(0.0, 0.0);
+                v[2 * u + c / 2][c % 2] = !MASK || e + c < len
+                                              ? to_f(*reinterpret_cast<const bf2*>(&w4[c]))
+                                              : cmake<M2>(0.0, 0.0);
         }
     } else if constexpr (std::is_same<C2, float2>::value) {
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
             const int e = pair_node<C2>(k);
             const float4 r = reinterpret_cast<const float4*>(tile)[threadIdx.x + kThreads * k];
-            v[k][0] = e < len ? make_double2(r.x, r.y) : make_double2(0.0, 0.0);
-            v[k][1] = e + 1 < len ? make_double2(r.z, r.w) : make_double2(0.0, 0.0);
+            v[k][0] = !MASK || e < len ? make_double2(r.x, r.y) : make_double2(0.0, 0.0);
+            v[k][1] = !MASK || e + 1 < len ? make_double2(r.z, r.w) : make_double2(0.0, 0.0);
         }
     } else {
 #pragma unroll
         for (int k = 0; k < kPairs; ++k) {
             const int e = pair_node<C2>(k);
             const double2* d = reinterpret_cast<const double2*>(tile) + e;
-            v[k][0] = e < len ? d[0] : make_double2(0.0, 0.0);
-            v[k][1] = e + 1 < len ? d[1] : make_double2(0.0, 0.0);
+            v[k][0] = !MASK || e < len ? d[0] : make_double2(0.0, 0.0);
+            v[k][1] = !MASK || e + 1 < len ? d[1] : make_double2(0.0, 0.0);
         }
     }
 }
 
-template <typename S>
+template <typename S, bool MS = false>
 __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long long N, GState g,
                                                                    int j, int proj) {
     using C2 = S;
     using P = OrthBulk<S>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
+    int nchunk = g.nchunk;
+    if constexpr (MS) {
+        N = g.slots[b].n;
+        nchunk = g.slots[b].nchunk;
+    }
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     if (proj) {
         if (cb.kc == 0) return;
@@ -1031,20 +1299,20 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
     }
     __syncthreads();  // hs, hm, barriers visible
     const int tpc = j + 2;  // tiles per chunk: w, u_0 .. u_j
-    const int nmy = int((g.nchunk - blockIdx.x + gridDim.x - 1) / gridDim.x);
+    const int nmy = nchunk > int(blockIdx.x) ? int((nchunk - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
     double acc = 0.0;
     if (warp == kThreads / 32) {
         // producer: one elected thread issues every tile of this CTA in order
         if (lane == 0) {
-            long long q = 0;
+            int q = 0;
             bool ok = true;
             for (int i = 0; i < nmy && ok; ++i) {
                 const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
                 const int len = int(min((long long)kChunk, N - n0));
                 const unsigned bytes = unsigned((size_t(len) * sizeof(C2) + 15) / 16 * 16);
                 for (int tt = 0; tt < tpc; ++tt, ++q) {
-                    const int s = int(q % P::STAGES);
-                    if (!mbar_wait(&empty[s], unsigned((q / P::STAGES) & 1) ^ 1u)) {
+                    const int s = q & (P::STAGES - 1);
+                    if (!mbar_wait(&empty[s], (unsigned(q >> P::LOG_STAGES) & 1u) ^ 1u)) {
                         ok = false;
                         break;
                     }
@@ -1061,11 +1329,11 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
             }
             // copies still in flight (none unless a wait ran out): the last
             // tile issued on each stage must land before the CTA leaves
-            for (long long r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
-                mbar_wait(&full[r % P::STAGES], unsigned((r / P::STAGES) & 1));
+            for (int r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
+                mbar_wait(&full[r & (P::STAGES - 1)], unsigned(r >> P::LOG_STAGES) & 1u);
         }
     } else {
-        long long q = 0;
+        int q = 0;
         for (int i = 0; i < nmy; ++i) {
             const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
             const int len = int(min((long long)kChunk, N - n0));
@@ -1074,14 +1342,19 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
 #pragma unroll
             for (int k = 0; k < kPairs; ++k) qacc[k][0] = qacc[k][1] = make_float2(0.f, 0.f);
             bool ok = true;
+            // Tail of a partial last chunk: complex64 / bfloat16 pairs that start
+            // before len lie in the copied bytes (rounded up into the zeroed
+            // padding), later ones are neither stored nor summed, so only
+            // complex128 (a node per 16 bytes) masks the values it reads.
+            constexpr bool MASK = std::is_same<C2, double2>::value;
             for (int tt = 0; tt < tpc; ++tt, ++q) {
-                const int s = int(q % P::STAGES);
-                if (!mbar_wait(&full[s], unsigned((q / P::STAGES) & 1))) {
+                const int s = q & (P::STAGES - 1);
+                if (!mbar_wait(&full[s], unsigned(q >> P::LOG_STAGES) & 1u)) {
                     ok = false;
                     break;
                 }
                 M2 v[kPairs][2];
-                tile_pairs<C2>(ring + size_t(s) * P::TILE, len, v);
+                tile_pairs<C2, MASK>(ring + size_t(s) * P::TILE, len, v);
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[s]);
                 if (tt == 0) {
@@ -1187,13 +1460,18 @@ __global__ void __launch_bounds__(128) k_lsq(GState g) {
 }
 
 // ------------------------------------------------------------ solution update
-template <typename S>
+template <typename S, bool MS = false>
 __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S* V, double2* x,
                                                      long long ld, GState g) {
     using C2 = S;
     using P = Pipe<C2>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
+    int nchunk = g.nchunk;
+    if constexpr (MS) {
+        op = g.slots[b].op64;
+        nchunk = g.slots[b].nchunk;
+    }
     extern __shared__ __align__(16) uint4 stg[];
     __shared__ double2 ys[USV_MAX_RESTART];
     __shared__ float2 yf[USV_MAX_RESTART];
@@ -1206,7 +1484,7 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
     // solution vectors: U_t (t < kc) of the cycle's pair, then Krylov slots
     const CycleBasis<C2> cb = cycle_basis(const_cast<C2*>(V), g, b);
     __syncthreads();  // ys visible
-    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
         double2 acc[kPairs][2];
@@ -1264,11 +1542,16 @@ template <> struct Wide<double2> { using T = double2; };
 // the host-read block. Each CTA stages a tile of U in shared memory; warp w
 // owns the slots s = w (mod warps) for every tile, so the per-CTA sums are
 // accumulated in a fixed order; the last CTA reduces the CTA partials.
-template <typename S, int K>
+template <typename S, int K, bool MS = false>
 __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g) {
     using T = typename Wide<S>::T;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
+    int nchunk = g.nchunk;
+    if constexpr (MS) {
+        N = g.slots[b].n;
+        nchunk = g.slots[b].nchunk;
+    }
     const CycleBasis<S> cb = cycle_basis(V, g, b);
     const int m = g.m;
     if (cb.kc != K) return;  // recycled cycles use all K vectors
@@ -1280,7 +1563,7 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
     for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) tab[q] = make_double2(0.0, 0.0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nw = kThreads / 32;
-    for (int ch = blockIdx.x; ch < g.nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
         for (int t0 = 0; t0 < kChunk; t0 += kBdTile) {
             const long long n0 = (long long)ch * kChunk + t0;
             const int len = int(max(0LL, min((long long)kBdTile, N - n0)));
@@ -1346,12 +1629,13 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
 // keeps the 2K outputs of kNpt nodes (coalesced, kThreads apart) in
 // registers; the shared coefficient row is read once per kNpt nodes.
 template <typename S> constexpr int kCombineNpt = sizeof(S) == 16 ? 1 : 2;
-template <typename S, int K>
+template <typename S, int K, bool MS = false>
 __global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState g) {
     using T = typename Wide<S>::T;
     constexpr int NPT = kCombineNpt<S>;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE) return;
+    if constexpr (MS) N = g.slots[b].n;
     const int* cw = g.ctl + b * kCtl;
     if (!cw[CW_COMBINE]) return;
     const int m = g.m, skc = cw[CW_SRC_KC];
@@ -1470,10 +1754,11 @@ __device__ __forceinline__ unsigned bf_pack(__nv_bfloat16 lo, __nv_bfloat16 hi) 
 static size_t combine_mma_smem(int k, int m) {
     return sizeof(uint2) * size_t((k + m + 1 + 7) / 8) * k * 32;
 }
-template <int K>
+template <int K, bool MS = false>
 __global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, GState g) {
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE) return;
+    if constexpr (MS) N = g.slots[b].n;
     const int* cw = g.ctl + b * kCtl;
     if (!cw[CW_COMBINE]) return;
     const int m = g.m, skc = cw[CW_SRC_KC];
@@ -1603,10 +1888,11 @@ __global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, G
 static size_t bdots_mma_smem(int k, int m) {
     return sizeof(double2) * (size_t(kThreads / 32) * 16 + size_t(m + 1)) * k;
 }
-template <int K>
+template <int K, bool MS = false>
 __global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GState g) {
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
+    if constexpr (MS) N = g.slots[b].n;
     const CycleBasis<bf2> cb = cycle_basis(V, g, b);
     const int m = g.m;
     if (cb.kc != K) return;  // recycled cycles use all K vectors
@@ -1718,10 +2004,11 @@ __global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GSt
 // ------------------------------------------------------------ final gates (fp64)
 // iterative_solver.py:70-79: ||R(OP x) - Rb|| / ||Rb|| and
 // max |OP x - b| / max(|OP||x| + |b|, 1e-30), plus a finiteness check.
-template <bool ADJ>
+template <bool ADJ, bool MS = false>
 __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2* rhs,
                                                const double2* x, long long ld, GState g) {
     const int b = blockIdx.y;
+    if constexpr (MS) op = g.slots[b].op64;
     __shared__ double sh[32];
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
@@ -1814,14 +2101,14 @@ struct EventHold {
 
 
 // The recycled-space kernels are instantiated for every k = 1..kMaxRecycle.
-template <typename S, int K> const void* recycle_kernel_k(bool combine) {
+template <typename S, int K, bool MS> const void* recycle_kernel_k(bool combine) {
     if constexpr (std::is_same<S, bf2>::value)
-        return combine ? (const void*)k_combine_mma<K> : (const void*)k_bdots_mma<K>;
-    return combine ? (const void*)k_combine<S, K> : (const void*)k_bdots<S, K>;
+        return combine ? (const void*)k_combine_mma<K, MS> : (const void*)k_bdots_mma<K, MS>;
+    return combine ? (const void*)k_combine<S, K, MS> : (const void*)k_bdots<S, K, MS>;
 }
-template <typename S> const void* recycle_kernel(int k, bool combine) {
+template <typename S, bool MS> const void* recycle_kernel(int k, bool combine) {
     switch (k) {
-#define USV_K(K) case K: return recycle_kernel_k<S, K>(combine);
+#define USV_K(K) case K: return recycle_kernel_k<S, K, MS>(combine);
         USV_K(1) USV_K(2) USV_K(3) USV_K(4) USV_K(5) USV_K(6) USV_K(7) USV_K(8)
         USV_K(9) USV_K(10) USV_K(11) USV_K(12) USV_K(13) USV_K(14) USV_K(15) USV_K(16)
 #undef USV_K
@@ -1903,21 +2190,28 @@ static bool recycle_coefficients(int m, int k, const double* hb, std::vector<dou
     return finite;
 }
 
-template <typename R, typename S, bool ADJ>
+template <typename R, typename S, bool ADJ, bool MS = false>
 static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_params& p,
                      const double2* rhs, double2* x, int B, long long ld, char* ws,
-                     const WsLayout& L, GState& g, usv_gmres_stats* stats, cudaStream_t strm) {
+                     const WsLayout& L, GState& g, usv_gmres_stats* stats, cudaStream_t strm,
+                     const std::vector<SceneSlot>* slots = nullptr) {
     using C2 = S;  // stored Krylov vector element
     const OpView<double> op64 = make_view<double>(s, op_buf, ADJ);
     const OpView<R> opk = make_view<R>(s, op_buf, ADJ);
     C2* V = reinterpret_cast<C2*>(ws + L.V);
+    if constexpr (MS) {
+        SceneSlot* dslots = reinterpret_cast<SceneSlot*>(ws + L.slots);
+        USV_CUDA_TRY(cudaMemcpyAsync(dslots, slots->data(), sizeof(SceneSlot) * size_t(B),
+                                     cudaMemcpyHostToDevice, strm));
+        g.slots = dslots;
+    }
     const size_t lsq_smem = sizeof(double2) * size_t(g.m) * (g.m + 1);
     const size_t pipe_smem = Pipe<C2>::STAGED ? Pipe<C2>::BYTES : 16;
     const Step step = make_step(kThreads, s.nx, s.ny);
     const Step step_d = make_step(kDotsThreads, s.nx, s.ny);
-    USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    USV_CUDA_TRY(cudaFuncSetAttribute(k_orth<S, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(pipe_smem)));
-    USV_CUDA_TRY(cudaFuncSetAttribute(k_update<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    USV_CUDA_TRY(cudaFuncSetAttribute(k_update<S, MS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(pipe_smem)));
     // Grids fill the GPU once (resident CTAs per SM x SMs, shared by the B
     // right-hand sides); every CTA loops over node chunks, so there is no
@@ -1935,19 +2229,41 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         return USV_OK;
     };
     dim3 grid_res, grid_dots, grid_orth, grid_upd, grid_gates;
-    if (int e = grid_for((const void*)k_residual<ADJ, C2>, 256, 0, grid_res)) return e;
-    if (int e = grid_for((const void*)k_dots<R, S, ADJ, kDotsThreads>, kDotsThreads, 0, grid_dots))
-        return e;
-    auto launch_dots = [&](cudaStream_t st, int j, int proj) {
-        k_dots<R, S, ADJ, kDotsThreads><<<grid_dots, kDotsThreads, 0, st>>>(opk, V, g, j, step_d, proj);
+    if (int e = grid_for((const void*)k_residual<ADJ, C2, MS>, 256, 0, grid_res)) return e;
+    // Arnoldi stencil + dots: per-warp dot tasks with direct loads (default;
+    // the bulk-copy tile ring of USV_GMRES_DOTS_BULK measured 15% slower at
+    // 128^3, its per-tile warp reductions cost more issue slots than the
+    // direct loads), always for complex128
+    const bool dots_warptask = (p.kernel_variant & USV_GMRES_DOTS_BULK) == 0;
+    const bool dots_bulk = !std::is_same<S, double2>::value && !dots_warptask;
+    const void* fn_dots = nullptr;
+    int dots_threads = kDotsThreads;
+    size_t dots_smem = 0;
+    if constexpr (!std::is_same<S, double2>::value) {
+        if (dots_bulk) {
+            fn_dots = (const void*)k_dots_bulk<R, S, ADJ, MS>;
+            dots_threads = DotsBulk<S>::THREADS;
+            dots_smem = DotsBulk<S>::smem(g.m);
+        }
+    }
+    if (!fn_dots) fn_dots = (const void*)k_dots<R, S, ADJ, kDotsThreads, MS>;
+    USV_CUDA_TRY(cudaFuncSetAttribute(fn_dots, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(dots_smem)));
+    if (int e = grid_for(fn_dots, dots_threads, dots_smem, grid_dots)) return e;
+    auto launch_dots = [&](cudaStream_t st, int j, int proj) -> cudaError_t {
+        OpView<R> ov = opk;
+        C2* vp = V;
+        GState gs = g;
+        Step sd = step_d;
+        void* args[] = {&ov, &vp, &gs, &j, &sd, &proj};
+        return cudaLaunchKernel(fn_dots, grid_dots, dim3(dots_threads), args, dots_smem, st);
     };
-    // orthogonalisation kernel: the bulk-copy ring (default) or the per-thread
-    // cp.async pipeline (USV_ORTH_KERNEL=cpasync)
-    static const bool orth_cpasync = [] {
-        const char* v = getenv("USV_ORTH_KERNEL");
-        return v && std::strcmp(v, "cpasync") == 0;
-    }();
-    const void* fn_orth = orth_cpasync ? (const void*)k_orth<S> : (const void*)k_orth_bulk<S>;
+    // orthogonalisation kernel: the bulk-copy ring (default for complex64 /
+    // bfloat16) or the per-thread pipeline (USV_GMRES_ORTH_CPASYNC; always for
+    // complex128, whose unrolled 16-byte loads need no staging)
+    const bool orth_cpasync = (p.kernel_variant & USV_GMRES_ORTH_CPASYNC) != 0 ||
+                              std::is_same<S, double2>::value;
+    const void* fn_orth = orth_cpasync ? (const void*)k_orth<S, MS> : (const void*)k_orth_bulk<S, MS>;
     const int orth_threads = orth_cpasync ? kThreads : OrthBulk<S>::THREADS;
     const size_t orth_smem = orth_cpasync ? pipe_smem : OrthBulk<S>::SMEM;
     USV_CUDA_TRY(cudaFuncSetAttribute(fn_orth, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1960,8 +2276,8 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         void* args[] = {&vp, &nn_, &gs, &j, &proj};
         return cudaLaunchKernel(fn_orth, grid_orth, dim3(orth_threads), args, orth_smem, st);
     };
-    if (int e = grid_for((const void*)k_update<S>, kThreads, pipe_smem, grid_upd)) return e;
-    if (int e = grid_for((const void*)k_gates<ADJ>, 256, 0, grid_gates)) return e;
+    if (int e = grid_for((const void*)k_update<S, MS>, kThreads, pipe_smem, grid_upd)) return e;
+    if (int e = grid_for((const void*)k_gates<ADJ, MS>, 256, 0, grid_gates)) return e;
     if (lsq_smem > 48 * 1024)
         USV_CUDA_TRY(cudaFuncSetAttribute(k_lsq, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(lsq_smem)));
@@ -1977,8 +2293,8 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
                       : sizeof(T) * size_t(kr) * kBdTile + sizeof(double2) * size_t(g.m + 1) * kr;
         comb_smem = std::is_same<S, bf2>::value ? combine_mma_smem(kr, g.m)
                                                 : sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
-        fn_bdots = recycle_kernel<S>(kr, false);
-        fn_comb = recycle_kernel<S>(kr, true);
+        fn_bdots = recycle_kernel<S, MS>(kr, false);
+        fn_comb = recycle_kernel<S, MS>(kr, true);
         if (!fn_bdots || !fn_comb) return USV_ERR_ARG;
         USV_CUDA_TRY(cudaFuncSetAttribute(fn_bdots, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(bd_smem)));
@@ -1992,6 +2308,10 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     if (kr > 0) {
         // Krylov and pair buffers start zero: every load stays finite, padding included
         USV_CUDA_TRY(cudaMemsetAsync(ws + L.V, 0, L.coef - L.V, strm));
+    } else if (MS) {
+        // scenes smaller than the vector stride: every vector is zero past its
+        // scene's last node (the same padding rule as below)
+        USV_CUDA_TRY(cudaMemsetAsync(ws + L.V, 0, L.partial - L.V, strm));
     } else if (g.nv > g.n) {
         // paired loads may touch the padding past node n-1 of each basis vector:
         // keep it zero so it contributes nothing to the dots
@@ -2000,7 +2320,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     }
     USV_CUDA_TRY(cudaMemset2DAsync(x, ld * sizeof(double2), 0, g.n * sizeof(double2), B, strm));
     if (kr == 0) {
-        k_residual<ADJ, C2><<<grid_res, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
+        k_residual<ADJ, C2, MS><<<grid_res, 256, 0, strm>>>(op64, rhs, x, ld, V, g, 1, step);
         USV_CUDA_TRY(cudaGetLastError());
     }
     // Recycling: pinned host blocks for the per-cycle read of the Hessenberg /
@@ -2029,7 +2349,14 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         ev.assign(kernels_per_cycle + 1, nullptr);
         for (auto& e : ev) USV_CUDA_TRY(cudaEventCreate(&e));
     }
-    const double vb = double(sizeof(C2)), nn = double(g.n);
+    // nodes per right-hand side for the byte counts (multi-scene: the mean)
+    double nn = double(g.n);
+    if constexpr (MS) {
+        nn = 0.0;
+        for (const SceneSlot& sl : *slots) nn += double(sl.n);
+        nn /= double(B);
+    }
+    const double vb = double(sizeof(C2));
     std::vector<double> fam_bytes;
     // per measured interval: the Arnoldi step j (-1: none) and whether it
     // only runs in recycled cycles (1) or with a new pair (2), so that the
@@ -2065,7 +2392,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam_shared.push_back(0.0);
             fam_step.push_back(-1);
             fam_need.push_back(2);
-            k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
+            k_residual<ADJ, C2, MS><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
             // per RHS: x, b, the stored residual; per launch: node record (R),
@@ -2074,7 +2401,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam_shared.push_back(nn * (sizeof(double4) + 7 * sizeof(double2)));
             fam_step.push_back(-1);
             fam_need.push_back(0);
-            launch_dots(st, 0, 1);
+            USV_CUDA_TRY(launch_dots(st, 0, 1));
             USV_CUDA_TRY(launch_orth(st, 0, 1));
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(7);
@@ -2084,7 +2411,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam_need.push_back(1);
         }
         for (int j = 0; j < g.m; ++j) {
-            launch_dots(st, j, 0);
+            USV_CUDA_TRY(launch_dots(st, j, 0));
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(0);
             // per RHS: read u_0..u_j (u_j also feeds the stencil), write w; per
@@ -2109,7 +2436,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
         fam_shared.push_back(0.0);
         fam_step.push_back(-1);
         fam_need.push_back(0);
-        k_update<S><<<grid_upd, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
+        k_update<S, MS><<<grid_upd, kThreads, pipe_smem, st>>>(op64, V, x, ld, g);
         USV_CUDA_TRY(mark(st, k++, capturing));
         fam.push_back(3);
         fam_bytes.push_back(nn * (vb * g.m + 2 * sizeof(double2) + sizeof(double4)));
@@ -2133,7 +2460,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
             fam_need.push_back(3);
             USV_CUDA_TRY(cudaMemcpyAsync(hb_pin.p, ws + L.hb, hb_bytes, cudaMemcpyDeviceToHost, st));
         } else {
-            k_residual<ADJ, C2><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
+            k_residual<ADJ, C2, MS><<<grid_res, 256, 0, st>>>(op64, rhs, x, ld, V, g, 0, step);
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(4);
             // per RHS: x, b, the stored residual; per launch: node record (R),
@@ -2279,7 +2606,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     }
     if (rc) return rc;
     if (prof) USV_CUDA_TRY(cudaEventRecord(ev[0], strm));
-    k_gates<ADJ><<<grid_gates, 256, 0, strm>>>(op64, rhs, x, ld, g);
+    k_gates<ADJ, MS><<<grid_gates, 256, 0, strm>>>(op64, rhs, x, ld, g);
     USV_CUDA_TRY(cudaGetLastError());
     if (prof) {
         USV_CUDA_TRY(cudaEventRecord(ev[1], strm));
@@ -2343,6 +2670,8 @@ static int check_params(const usv_scene* scene, const usv_gmres_params* p, int n
         return USV_ERR_ARG;
     *m = int(p->restart < *n ? p->restart : *n);
     if (p->recycle < 0 || p->recycle_every < 0) return USV_ERR_ARG;
+    if (p->max_ctas < 0 || (p->kernel_variant & ~(USV_GMRES_ORTH_CPASYNC | USV_GMRES_DOTS_BULK)))
+        return USV_ERR_ARG;
     if (p->recycle > 0 && (p->recycle > kMaxRecycle || p->recycle > *m - 1)) return USV_ERR_ARG;
     *chunk = kChunk;  // node chunk per CTA (block_nodes is reserved)
     if (p->block_nodes != 0 && p->block_nodes != kChunk) return USV_ERR_ARG;
@@ -2353,6 +2682,58 @@ static int check_params(const usv_scene* scene, const usv_gmres_params* p, int n
 }  // namespace usv
 
 using namespace usv;
+
+// Device state of one solve inside the caller's workspace.
+static GState make_state(char* ws, const WsLayout& L, const usv_gmres_params* params, long long n,
+                         int m, int chunk, int nblk, int nrhs) {
+    const int kr = params->recycle;
+    GState g{};
+    g.m = m;
+    g.nblk = nblk;
+    g.nchunk = nblk;
+    g.chunk = chunk;
+    g.full_cycles = params->full_cycles ? 1 : 0;
+    g.maxiter = params->maxiter;
+    g.n = n;
+    g.nv = padded(n);
+    g.rtol = params->rtol;
+    g.partial = reinterpret_cast<double2*>(ws + L.partial);
+    g.H = reinterpret_cast<double2*>(ws + L.H);
+    g.gc = reinterpret_cast<double*>(ws + L.gc);
+    g.gs = reinterpret_cast<double2*>(ws + L.gs);
+    g.g = reinterpret_cast<double2*>(ws + L.g);
+    g.y = reinterpret_cast<double2*>(ws + L.y);
+    g.sigma = reinterpret_cast<double*>(ws + L.sigma);
+    g.bnorm = reinterpret_cast<double*>(ws + L.bnorm);
+    g.atol = reinterpret_cast<double*>(ws + L.atol);
+    g.wnorm = reinterpret_cast<double*>(ws + L.wnorm);
+    g.gates = reinterpret_cast<double*>(ws + L.gates);
+    g.hist = reinterpret_cast<double*>(ws + L.hist);
+    g.hcap = params->history_capacity > 0 ? params->history_capacity : 0;
+    g.status = reinterpret_cast<int*>(ws + L.status);
+    g.cycles = reinterpret_cast<int*>(ws + L.cycles);
+    g.iters = reinterpret_cast<int*>(ws + L.iters);
+    g.len = reinterpret_cast<int*>(ws + L.len);
+    g.ended = reinterpret_cast<int*>(ws + L.ended);
+    g.counter = reinterpret_cast<unsigned*>(ws + L.counter);
+    g.ps = partial_slots(m, kr);
+    g.kr = kr;
+    if (kr > 0) {
+        g.hb_len = hb_size(m, kr);
+        g.vstride = (long long)nrhs * (m + 1) * g.nv;
+        g.pstride = (long long)nrhs * kr * g.nv;
+        g.Ubuf = ws + L.U;
+        g.Cbuf = ws + L.C;
+        g.ctl = reinterpret_cast<int*>(ws + L.ctl);
+        g.coef = reinterpret_cast<double2*>(ws + L.coef);
+        g.hb = reinterpret_cast<double*>(ws + L.hb);
+        g.dU = reinterpret_cast<double*>(ws + L.dU);
+        g.alpha = reinterpret_cast<double2*>(ws + L.alpha);
+        g.klast = reinterpret_cast<int*>(ws + L.klast);
+        g.started = reinterpret_cast<int*>(ws + L.started);
+    }
+    return g;
+}
 
 extern "C" {
 
@@ -2402,56 +2783,104 @@ int usv_gmres_solve(const usv_scene* scene, const void* op_buf, const usv_gmres_
     const WsLayout L = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity, kr);
     if (workspace_bytes < L.total) return USV_ERR_WORKSPACE;
     char* ws = static_cast<char*>(workspace);
-    GState g{};
-    g.m = m;
-    g.nblk = nblk;
-    g.nchunk = nblk;
-    g.chunk = chunk;
-    g.full_cycles = params->full_cycles ? 1 : 0;
-    g.maxiter = params->maxiter;
-    g.n = n;
-    g.nv = padded(n);
-    g.rtol = params->rtol;
-    g.partial = reinterpret_cast<double2*>(ws + L.partial);
-    g.H = reinterpret_cast<double2*>(ws + L.H);
-    g.gc = reinterpret_cast<double*>(ws + L.gc);
-    g.gs = reinterpret_cast<double2*>(ws + L.gs);
-    g.g = reinterpret_cast<double2*>(ws + L.g);
-    g.y = reinterpret_cast<double2*>(ws + L.y);
-    g.sigma = reinterpret_cast<double*>(ws + L.sigma);
-    g.bnorm = reinterpret_cast<double*>(ws + L.bnorm);
-    g.atol = reinterpret_cast<double*>(ws + L.atol);
-    g.wnorm = reinterpret_cast<double*>(ws + L.wnorm);
-    g.gates = reinterpret_cast<double*>(ws + L.gates);
-    g.hist = reinterpret_cast<double*>(ws + L.hist);
-    g.hcap = params->history_capacity > 0 ? params->history_capacity : 0;
-    g.status = reinterpret_cast<int*>(ws + L.status);
-    g.cycles = reinterpret_cast<int*>(ws + L.cycles);
-    g.iters = reinterpret_cast<int*>(ws + L.iters);
-    g.len = reinterpret_cast<int*>(ws + L.len);
-    g.ended = reinterpret_cast<int*>(ws + L.ended);
-    g.counter = reinterpret_cast<unsigned*>(ws + L.counter);
-    g.ps = partial_slots(m, kr);
-    g.kr = kr;
-    if (kr > 0) {
-        g.hb_len = hb_size(m, kr);
-        g.vstride = (long long)nrhs * (m + 1) * g.nv;
-        g.pstride = (long long)nrhs * kr * g.nv;
-        g.Ubuf = ws + L.U;
-        g.Cbuf = ws + L.C;
-        g.ctl = reinterpret_cast<int*>(ws + L.ctl);
-        g.coef = reinterpret_cast<double2*>(ws + L.coef);
-        g.hb = reinterpret_cast<double*>(ws + L.hb);
-        g.dU = reinterpret_cast<double*>(ws + L.dU);
-        g.alpha = reinterpret_cast<double2*>(ws + L.alpha);
-        g.klast = reinterpret_cast<int*>(ws + L.klast);
-        g.started = reinterpret_cast<int*>(ws + L.started);
-    }
+    GState g = make_state(ws, L, params, n, m, chunk, nblk, nrhs);
     cudaStream_t strm = static_cast<cudaStream_t>(stream);
     const double2* b = static_cast<const double2*>(rhs);
     double2* xx = static_cast<double2*>(x);
     const bool adj = params->adjoint != 0;
 #define USV_RUN(R, S, A) run_gmres<R, S, A>(*scene, op_buf, *params, b, xx, nrhs, ld, ws, L, g, stats, strm)
+    if (params->precision == USV_PREC_FP64)
+        return adj ? USV_RUN(double, double2, true) : USV_RUN(double, double2, false);
+    if (params->precision == USV_PREC_MIXED_BF16)
+        return adj ? USV_RUN(float, bf2, true) : USV_RUN(float, bf2, false);
+    return adj ? USV_RUN(float, float2, true) : USV_RUN(float, float2, false);
+#undef USV_RUN
+}
+
+
+// Several scenes in one batched solve: right-hand side b belongs to scene
+// scene_of_rhs[b] (operator buffer op_bufs[scene]); every launch of a cycle
+// covers all right-hand sides of all scenes, each CTA row (blockIdx.y = b)
+// reading its scene from the slot table in the workspace. Vectors are laid
+// out for the largest scene (ld >= its node count); a right-hand side of a
+// smaller scene uses the first n entries of its column.
+static int check_scenes(int nscenes, const usv_scene* scenes, const void* const* op_bufs,
+                        const int* scene_of_rhs, const usv_gmres_params* params, int nrhs,
+                        long long* nmax, int* m, int* chunk, int* nblk) {
+    if (nscenes < 1 || !scenes || !scene_of_rhs || !params || nrhs < 1) return USV_ERR_ARG;
+    *nmax = 0;
+    int mmin = 1 << 30;
+    for (int sc = 0; sc < nscenes; ++sc) {
+        long long n;
+        int mi, ch, nb;
+        if (int st = check_params(&scenes[sc], params, nrhs, &n, &mi, &ch, &nb)) return st;
+        if (op_bufs && !op_bufs[sc]) return USV_ERR_ARG;
+        if (n > *nmax) *nmax = n;
+        if (mi < mmin) mmin = mi;
+        *chunk = ch;
+    }
+    for (int b = 0; b < nrhs; ++b)
+        if (scene_of_rhs[b] < 0 || scene_of_rhs[b] >= nscenes) return USV_ERR_ARG;
+    // one restart length for the batch: every scene must allow the requested m
+    if (mmin != (params->restart < *nmax ? params->restart : int(*nmax))) return USV_ERR_ARG;
+    *m = mmin;
+    *nblk = int((*nmax + *chunk - 1) / *chunk);
+    return USV_OK;
+}
+
+int usv_gmres_scenes_workspace_bytes(int nscenes, const usv_scene* scenes,
+                                     const int* scene_of_rhs, const usv_gmres_params* params,
+                                     int nrhs, size_t* bytes) {
+    long long n;
+    int m, chunk, nblk;
+    int st = check_scenes(nscenes, scenes, nullptr, scene_of_rhs, params, nrhs, &n, &m, &chunk, &nblk);
+    if (st) return st;
+    if (!bytes) return USV_ERR_ARG;
+    *bytes = ws_layout(n, m, nrhs, nblk, vector_bytes(params->precision), params->history_capacity,
+                       params->recycle).total;
+    return USV_OK;
+}
+
+int usv_gmres_solve_scenes(int nscenes, const usv_scene* scenes, const void* const* op_bufs,
+                           const int* scene_of_rhs, const usv_gmres_params* params,
+                           const void* rhs, void* x, int nrhs, int64_t ld, void* workspace,
+                           size_t workspace_bytes, usv_gmres_stats* stats, void* stream) {
+    long long n;
+    int m, chunk, nblk;
+    int st = check_scenes(nscenes, scenes, op_bufs, scene_of_rhs, params, nrhs, &n, &m, &chunk,
+                          &nblk);
+    if (st) return st;
+    if (!op_bufs || !rhs || !x || !workspace || !stats || ld < n) return USV_ERR_ARG;
+    const size_t vb = vector_bytes(params->precision);
+    const WsLayout L = ws_layout(n, m, nrhs, nblk, vb, params->history_capacity, params->recycle);
+    if (workspace_bytes < L.total) return USV_ERR_WORKSPACE;
+    char* ws = static_cast<char*>(workspace);
+    GState g = make_state(ws, L, params, n, m, chunk, nblk, nrhs);
+    const bool adj = params->adjoint != 0;
+    std::vector<SceneSlot> slots(nrhs);
+    for (int b = 0; b < nrhs; ++b) {
+        const usv_scene& sc = scenes[scene_of_rhs[b]];
+        const void* buf = op_bufs[scene_of_rhs[b]];
+        SceneSlot& sl = slots[b];
+        sl.op64 = make_view<double>(sc, buf, adj);
+        sl.op32 = make_view<float>(sc, buf, adj);
+        sl.n = (long long)sc.nx * sc.ny * sc.nz;
+        sl.nchunk = int((sl.n + chunk - 1) / chunk);
+        sl.step = make_step(kThreads, sc.nx, sc.ny);
+        sl.step_d = make_step(kDotsThreads, sc.nx, sc.ny);
+    }
+    // the zeroing of the solution covers each column's own scene
+    cudaStream_t strm = static_cast<cudaStream_t>(stream);
+    const double2* b = static_cast<const double2*>(rhs);
+    double2* xx = static_cast<double2*>(x);
+    // the driver's scene-level set-up (grids, workspace clearing) uses the
+    // largest scene; kernels take each right-hand side's own scene
+    int big = 0;
+    for (int sc = 1; sc < nscenes; ++sc)
+        if ((long long)scenes[sc].nx * scenes[sc].ny * scenes[sc].nz >
+            (long long)scenes[big].nx * scenes[big].ny * scenes[big].nz)
+            big = sc;
+#define USV_RUN(R, S, A) run_gmres<R, S, A, true>(scenes[big], op_bufs[big], *params, b, xx, nrhs, ld, ws, L, g, stats, strm, &slots)
     if (params->precision == USV_PREC_FP64)
         return adj ? USV_RUN(double, double2, true) : USV_RUN(double, double2, false);
     if (params->precision == USV_PREC_MIXED_BF16)

@@ -361,6 +361,115 @@ __global__ void __launch_bounds__(kZTX * kZTY) k_apply_k25(OpView<R> op, const t
                         [&](long long n, typename Tr<R>::c2 v) { yb[n] = v; });
 }
 
+// y = K x (K' x) in complex64 for up to NB right-hand sides from the 16-byte
+// node records {rho, R, s}: the operator data a batch reads is 16 B per node
+// (the coefficients are formed in registers: harmonic densities, face
+// products of the 1-D tables, row scale and neighbour Jacobi), plus 8 B of x
+// and 8 B of y per node and right-hand side. z-marching tile (2.5-D
+// blocking): a CTA owns a 32 x 8 tile of (i, j) columns and the planes
+// [z0, z1); each thread keeps its column's record and values at z-1 .. z+2 in
+// registers (two planes of prefetch) and the halo node of its tile edge one
+// plane ahead; the x/y neighbours of plane z come from a double-buffered
+// shared-memory tile with a one-node halo (one barrier per plane). Each
+// thread forms its row's six coefficients once and applies them to every
+// right-hand side.
+template <int NB, bool ADJ>
+__global__ void __launch_bounds__(kZTX * kZTY) k_apply_rec25(OpView<float> op,
+                                                             const float2* __restrict__ x,
+                                                             float2* __restrict__ y, long long ld,
+                                                             int nrhs, int zseg) {
+    __shared__ float4 srec[2][kZTY + 2][kZTX + 2];
+    __shared__ float2 su[2][NB][kZTY + 2][kZTX + 2];
+    const int tiles_x = (op.nx + kZTX - 1) / kZTX;
+    const int bx = blockIdx.x % tiles_x, by = blockIdx.x / tiles_x;
+    const int tx = threadIdx.x % kZTX, ty = threadIdx.x / kZTX;
+    const int i = bx * kZTX + tx, j = by * kZTY + ty;
+    const bool in = i < op.nx && j < op.ny;
+    const int z0 = blockIdx.y * zseg, z1 = min(op.nz, z0 + zseg);
+    const long long sz = (long long)op.nx * op.ny;
+    auto load = [&](int ii, int jj, int z, float4& r, float2 (&v)[NB]) {
+        if (ii >= 0 && ii < op.nx && jj >= 0 && jj < op.ny && z >= 0 && z < op.nz) {
+            const long long n = ii + (long long)op.nx * jj + sz * z;
+            r = __ldg(op.rec + n);
+#pragma unroll
+            for (int b = 0; b < NB; ++b)
+                v[b] = b < nrhs ? __ldg(x + b * ld + n) : make_float2(0.f, 0.f);
+        } else {
+            r = make_float4(1.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) v[b] = make_float2(0.f, 0.f);
+        }
+    };
+    const int hxi = tx == 0 ? i - 1 : (tx == kZTX - 1 ? i + 1 : -2);
+    const int hyj = ty == 0 ? j - 1 : (ty == kZTY - 1 ? j + 1 : -2);
+    const int hxs = tx == 0 ? 0 : kZTX + 1, hys = ty == 0 ? 0 : kZTY + 1;
+    float4 rp, rc, r1, r2, hxr, hyr, hxr1, hyr1;
+    float2 up[NB], uc[NB], u1[NB], u2[NB], hxu[NB], hyu[NB], hxu1[NB], hyu1[NB];
+    load(i, j, z0 - 1, rp, up);
+    load(i, j, z0, rc, uc);
+    load(i, j, z0 + 1, r1, u1);
+    if (hxi != -2) load(hxi, j, z0, hxr, hxu);
+    if (hyj != -2) load(i, hyj, z0, hyr, hyu);
+    for (int z = z0; z < z1; ++z) {
+        load(i, j, z + 2, r2, u2);
+        if (hxi != -2) load(hxi, j, z + 1, hxr1, hxu1);
+        if (hyj != -2) load(i, hyj, z + 1, hyr1, hyu1);
+        const int bf = (z - z0) & 1;
+        srec[bf][ty + 1][tx + 1] = rc;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) su[bf][b][ty + 1][tx + 1] = uc[b];
+        if (hxi != -2) {
+            srec[bf][ty + 1][hxs] = hxr;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) su[bf][b][ty + 1][hxs] = hxu[b];
+        }
+        if (hyj != -2) {
+            srec[bf][hys][tx + 1] = hyr;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) su[bf][b][hys][tx + 1] = hyu[b];
+        }
+        __syncthreads();  // plane z visible; the other buffer was last read two planes ago
+        if (in) {
+            const Node p{i, j, z};
+            float2 c[6];
+            k_coefs_from<ADJ>(op, p, rc, [&](int dir) {
+                switch (dir) {
+                    case 0: return srec[bf][ty + 1][tx];
+                    case 1: return srec[bf][ty + 1][tx + 2];
+                    case 2: return srec[bf][ty][tx + 1];
+                    case 3: return srec[bf][ty + 2][tx + 1];
+                    case 4: return rp;
+                    default: return r1;
+                }
+            }, c);
+            const long long n = i + (long long)op.nx * j + sz * z;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                if (b >= nrhs) break;
+                float2 v = uc[b];
+                auto mac = [&](float2 cd, float2 u) {
+                    v.x = fmaf(cd.x, u.x, fmaf(-cd.y, u.y, v.x));
+                    v.y = fmaf(cd.x, u.y, fmaf(cd.y, u.x, v.y));
+                };
+                mac(c[0], su[bf][b][ty + 1][tx]);
+                mac(c[1], su[bf][b][ty + 1][tx + 2]);
+                mac(c[2], su[bf][b][ty][tx + 1]);
+                mac(c[3], su[bf][b][ty + 2][tx + 1]);
+                mac(c[4], up[b]);
+                mac(c[5], u1[b]);
+                y[b * ld + n] = v;
+            }
+        }
+        rp = rc; rc = r1; r1 = r2;
+        hxr = hxr1; hyr = hyr1;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            up[b] = uc[b]; uc[b] = u1[b]; u1[b] = u2[b];
+            hxu[b] = hxu1[b]; hyu[b] = hyu1[b];
+        }
+    }
+}
+
 __global__ void k_export(OpView<double> f, OpView<double> a, double* diag, double* rs,
                          double* jac, double* rsa, double* jaca) {
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < f.n;
@@ -484,7 +593,15 @@ int usv_operator_build(const usv_scene* scene, const double* rho, const double* 
 
 int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant, int precision,
                        const void* x, void* y, int nrhs, int64_t ld, void* stream) {
+    return usv_operator_apply_kernel(scene, op_buf, variant, precision, USV_STENCIL_AUTO, x, y,
+                                     nrhs, ld, stream);
+}
+
+int usv_operator_apply_kernel(const usv_scene* scene, const void* op_buf, int variant,
+                              int precision, int kernel, const void* x, void* y, int nrhs,
+                              int64_t ld, void* stream) {
     if (!scene || !op_buf || !x || !y || nrhs < 1 || nrhs > 65535) return USV_ERR_ARG;
+    if (kernel < USV_STENCIL_AUTO || kernel > USV_STENCIL_RECORD_TILES) return USV_ERR_ARG;
     const usv_scene& s = *scene;
     const long long n = (long long)s.nx * s.ny * s.nz;
     if (ld < n) return USV_ERR_ARG;
@@ -526,7 +643,24 @@ int usv_operator_apply(const usv_scene* scene, const void* op_buf, int variant, 
                 else k_apply_k25<double, false><<<g25, kZTX * kZTY, 0, strm>>>(v, (const double2*)x, (double2*)y, ld, zg.zseg);
             } else if (precision == USV_PREC_MIXED) {
                 auto v = make_view<float>(s, op_buf, adj);
-                if (nrhs <= 8 && s.nz <= 65535) {
+                if (kernel == USV_STENCIL_RECORD_TILES && nrhs > 4) return USV_ERR_ARG;
+                if (kernel == USV_STENCIL_RECORD_TILES) {
+                    const int r = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : 4;
+                    int dev = 0, sms = 148, per_sm = 1;
+                    cudaGetDevice(&dev);
+                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                    const void* fn = nullptr;
+                    if (r == 1) fn = adj ? (const void*)k_apply_rec25<1, true> : (const void*)k_apply_rec25<1, false>;
+                    else if (r == 2) fn = adj ? (const void*)k_apply_rec25<2, true> : (const void*)k_apply_rec25<2, false>;
+                    else fn = adj ? (const void*)k_apply_rec25<4, true> : (const void*)k_apply_rec25<4, false>;
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kZTX * kZTY, 0);
+                    const ZGrid zg = zmarch_grid(s.nx, s.ny, s.nz, (per_sm > 0 ? per_sm : 1) * sms);
+                    const float2* xf = (const float2*)x;
+                    float2* yf = (float2*)y;
+                    int zseg = zg.zseg;
+                    void* args[] = {&v, &xf, &yf, &ld, &nrhs, &zseg};
+                    USV_CUDA_TRY(cudaLaunchKernel(fn, dim3(zg.tiles, zg.runs), dim3(kZTX * kZTY), args, 0, strm));
+                } else if (nrhs <= 8 && s.nz <= 65535) {
                     const float2* xf = (const float2*)x;
                     float2* yf = (float2*)y;
                     const int r = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : 8;

@@ -89,8 +89,15 @@ template <> __device__ __forceinline__ double2 from_d<double2>(double2 a) { retu
 // bfloat16 complex storage of Krylov vectors (USV_PREC_MIXED_BF16): 4 bytes per
 // value, widened to float for the stencil and to double for the dots.
 using bf2 = __nv_bfloat162;
+// bfloat16 -> fp32 is exact: the 16 bits are the high half of the fp32 word,
+// so the packed pair {lo, hi} widens with one shift and one mask (integer
+// pipe) instead of two conversion instructions.
+__device__ __forceinline__ float2 bf2_to_f2(bf2 a) {
+    const unsigned u = *reinterpret_cast<const unsigned*>(&a);
+    return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+}
 __device__ __forceinline__ double2 to_d(bf2 a) {
-    const float2 f = __bfloat1622float2(a);
+    const float2 f = bf2_to_f2(a);
     return make_double2(f.x, f.y);
 }
 template <> __device__ __forceinline__ bf2 from_d<bf2>(double2 a) {
@@ -100,7 +107,7 @@ template <> __device__ __forceinline__ bf2 from_d<bf2>(double2 a) {
 template <typename C> __device__ __forceinline__ C widen(float2 a) { return cmake<C>(a.x, a.y); }
 template <typename C> __device__ __forceinline__ C widen(double2 a) { return cmake<C>(a.x, a.y); }
 template <typename C> __device__ __forceinline__ C widen(bf2 a) {
-    const float2 f = __bfloat1622float2(a);
+    const float2 f = bf2_to_f2(a);
     return cmake<C>(f.x, f.y);
 }
 template <> __device__ __forceinline__ float2 widen<float2>(float2 a) { return a; }
@@ -329,6 +336,49 @@ __device__ __forceinline__ typename Tr<R>::c2 k_row_from(const OpView<R>& op, No
         edge(5, cmul(fxy, op.Q[2][p.k]),
              ADJ && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
     return cadd(un, cscale(acc, me.y));
+}
+
+// The six coefficients c_d of the complex64 row of K (K') at node p from the
+// 16-byte node records {rho, R, s.re, s.im}: c_d = R_n e_nd s_d with
+// e_nd = F_d 2/(rho_n + rho_d) (conj(e_nd) for K'), zero for a missing
+// neighbour, for a fixed neighbour of an adjoint row and for every edge of a
+// fixed forward row, so that y = u_n + sum_d c_d u_d. rec(dir) returns the
+// neighbour record in direction dir = 0..5 (x-, x+, y-, y+, z-, z+); it is
+// never called for a direction outside the grid.
+template <bool ADJ, typename Rec>
+__device__ __forceinline__ void k_coefs_from(const OpView<float>& op, Node p, float4 me, Rec&& rec,
+                                             float2 (&c)[6]) {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) c[d] = make_float2(0.f, 0.f);
+    const bool fixed = node_fixed(op.soft, p.i, p.j, p.k, op.nx, op.ny, op.nz);
+    if (!ADJ && fixed) return;
+    const float2 tx = op.T[0][p.i], ty = op.T[1][p.j], tz = op.T[2][p.k];
+    const float2 fyz = cmul(ty, tz), fxz = cmul(tx, tz), fxy = cmul(tx, ty);
+    auto edge = [&](int dir, float2 F, bool nb_fixed) {
+        if (ADJ && nb_fixed) return;
+        const float4 r = rec(dir);
+        float2 e = cscale(F, harmonic2<float>(me.x, r.x) * me.y);
+        if (ADJ) e = cconj(e);
+        c[dir] = cmul(e, make_float2(r.z, r.w));
+    };
+    if (p.i > 0)
+        edge(0, cmul(fyz, op.Q[0][p.i - 1]),
+             ADJ && node_fixed(op.soft, p.i - 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.i < op.nx - 1)
+        edge(1, cmul(fyz, op.Q[0][p.i]),
+             ADJ && node_fixed(op.soft, p.i + 1, p.j, p.k, op.nx, op.ny, op.nz));
+    if (p.j > 0)
+        edge(2, cmul(fxz, op.Q[1][p.j - 1]),
+             ADJ && node_fixed(op.soft, p.i, p.j - 1, p.k, op.nx, op.ny, op.nz));
+    if (p.j < op.ny - 1)
+        edge(3, cmul(fxz, op.Q[1][p.j]),
+             ADJ && node_fixed(op.soft, p.i, p.j + 1, p.k, op.nx, op.ny, op.nz));
+    if (p.k > 0)
+        edge(4, cmul(fxy, op.Q[2][p.k - 1]),
+             ADJ && node_fixed(op.soft, p.i, p.j, p.k - 1, op.nx, op.ny, op.nz));
+    if (p.k < op.nz - 1)
+        edge(5, cmul(fxy, op.Q[2][p.k]),
+             ADJ && node_fixed(op.soft, p.i, p.j, p.k + 1, op.nx, op.ny, op.nz));
 }
 
 // Complex64 row from the precomputed coefficients (operator.cu: k_coef):

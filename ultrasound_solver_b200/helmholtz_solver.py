@@ -145,6 +145,7 @@ class HelmholtzB200Solver:
             recycle_every=int(s.get("gmres_recycle_every", 1)),
             batch_width=int(s.get("gmres_batch_width", 0)),
             max_ctas=int(s.get("gmres_max_ctas", 0)),
+            kernel_variant=int(s.get("gmres_kernel_variant", 0)),
         )
 
     # ----------------------------------------------------------- scene

@@ -42,7 +42,8 @@ class B200IterativeSolver:
                  backward_error_tol: float = 1.0e-4, precision: str = "mixed",
                  full_cycles: bool = True, use_graph: bool = True, block_nodes: int = 0,
                  verbose: bool = False, profile: bool = False, recycle: int = 0,
-                 recycle_every: int = 1, batch_width: int = 0, max_ctas: int = 0):
+                 recycle_every: int = 1, batch_width: int = 0, max_ctas: int = 0,
+                 kernel_variant: int = 0):
         if str(precision).lower() not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         self.restart = int(restart)
@@ -60,6 +61,9 @@ class B200IterativeSolver:
         # cap on CTAs per right-hand side (0: fill the GPU); a small cap makes
         # every CTA of the streaming kernels loop over several node chunks
         self.max_ctas = int(max_ctas)
+        # N.GMRES_* bits selecting other forms of the Arnoldi kernels than the
+        # measured-fastest default (autotune.BatchTuner can pick them)
+        self.kernel_variant = int(kernel_variant)
         self.verbose = bool(verbose)
         self.profile = bool(profile)
         self.last_profile = None
@@ -85,6 +89,7 @@ class B200IterativeSolver:
         p.recycle = self.recycle
         p.recycle_every = self.recycle_every
         p.max_ctas = self.max_ctas
+        p.kernel_variant = self.kernel_variant
         return p
 
     def workspace_bytes(self, operator, nrhs: int, adjoint: bool = False) -> int:
@@ -149,6 +154,13 @@ class B200IterativeSolver:
                                              N.stream_handle(torch, operator.device)),
                     "gmres")
         del ws
+        self.record_stats(stats, hist, hcap, prof, raise_on_failure)
+        return x
+
+    def record_stats(self, stats, hist, hcap, prof, raise_on_failure: bool) -> None:
+        """Per-RHS statistics of a finished launch (last_stats, last_history,
+        last_profile, the maxima over the batch); raises the reference's
+        RuntimeError for a right-hand side that failed its gates."""
         self.last_stats = [dict(status=s.status, info=s.info, iterations=s.iterations,
                                 cycles=s.cycles, scaled_residual=s.scaled_residual,
                                 backward_error=s.backward_error,
@@ -174,4 +186,3 @@ class B200IterativeSolver:
             print(f"  --> GMRES iterations: {self.last_iterations} | scaled relative residual: "
                   f"{self.last_scaled_residual:.3e} | backward error: "
                   f"{self.last_backward_error:.3e}")
-        return x

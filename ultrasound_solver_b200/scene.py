@@ -122,6 +122,7 @@ class DeviceOperator:
                 and bool((rho > 0).all()) and bool((c > 0).all())):
             raise ValueError("density and sound speed must be finite and positive")
         self.device = rho.device
+        self.stencil_kernel = N.STENCIL_AUTO
         self.rho = rho.to(torch.float64).contiguous()
         self.c = c.to(torch.float64).contiguous()
         lib = N.load()
@@ -148,8 +149,12 @@ class DeviceOperator:
     def fixed_dofs(self) -> np.ndarray:
         return np.flatnonzero(self.fixed_mask.ravel(order="F"))
 
-    def apply(self, x: torch.Tensor, variant: int = N.APPLY_A, precision: int = N.PREC_FP64):
-        """y = OP x for x of shape (N,) or (B, N) (complex128; complex64 allowed for K/KH mixed)."""
+    def apply(self, x: torch.Tensor, variant: int = N.APPLY_A, precision: int = N.PREC_FP64,
+              kernel: int | None = None):
+        """y = OP x for x of shape (N,) or (B, N) (complex128; complex64 allowed for K/KH mixed).
+
+        `kernel` selects the complex64 K / K^H stencil (N.STENCIL_*); None
+        uses `self.stencil_kernel` (set by autotune.StencilTuner, default auto)."""
         squeeze = x.dim() == 1
         xb = x.reshape(1, -1) if squeeze else x
         if xb.shape[-1] != self.n:
@@ -158,9 +163,13 @@ class DeviceOperator:
                                    and precision == N.PREC_MIXED) else torch.complex128
         xb = xb.to(device=self.device, dtype=want).contiguous()
         y = torch.empty_like(xb)
-        N.check(N.load().usv_operator_apply(C.byref(self.scene), N.ptr(self.buffer), variant,
-                                            precision, N.ptr(xb), N.ptr(y), xb.shape[0], self.n,
-                                            N.stream_handle(torch, self.device)), "apply")
+        k = self.stencil_kernel if kernel is None else int(kernel)
+        if k == N.STENCIL_RECORD_TILES and xb.shape[0] > 4:
+            k = N.STENCIL_AUTO  # the record-tile kernel takes at most 4 right-hand sides
+        N.check(N.load().usv_operator_apply_kernel(C.byref(self.scene), N.ptr(self.buffer), variant,
+                                                   precision, k, N.ptr(xb), N.ptr(y), xb.shape[0],
+                                                   self.n, N.stream_handle(torch, self.device)),
+                "apply")
         return y[0] if squeeze else y
 
     def export(self):
