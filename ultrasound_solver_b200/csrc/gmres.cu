@@ -161,6 +161,8 @@ static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes,
         L.ctl = take(sizeof(int) * size_t(B) * kCtl);
     }
     L.partial = take(sizeof(double2) * size_t(B) * nblk * partial_slots(m, k));
+    // (before state_begin: the driver clears the state after uploading the slots)
+    L.slots = take(sizeof(SceneSlot) * size_t(B));
     L.state_begin = off;
     L.H = take(sizeof(double2) * size_t(B) * m * (m + 1));
     L.gc = take(sizeof(double) * size_t(B) * m);
@@ -185,7 +187,6 @@ static WsLayout ws_layout(long long n, int m, int B, int nblk, size_t vec_bytes,
         L.klast = take(sizeof(int) * B);
         L.started = take(sizeof(int) * B);
     }
-    L.slots = take(sizeof(SceneSlot) * size_t(B));
     L.total = off;
     return L;
 }
@@ -1212,7 +1213,7 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
 template <typename S> struct OrthBulk {
     static constexpr int TILE = kChunk * int(sizeof(S));   // bytes per chunk tile
     // stages: a power of two (ring index and phase by mask and shift)
-    static constexpr int LOG_STAGES = sizeof(S) == 4 ? 3 : 2;
+    static constexpr int LOG_STAGES = 2;
     static constexpr int STAGES = 1 << LOG_STAGES;
     static constexpr size_t SMEM = size_t(STAGES) * TILE + 2 * STAGES * sizeof(unsigned long long);
     static constexpr int THREADS = kThreads + 32;           // + the producer warp
@@ -1338,9 +1339,6 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
             const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
             const int len = int(min((long long)kChunk, N - n0));
             M2 u[kPairs][2];
-            float2 qacc[kPairs][2];  // bfloat16: the (Im, Re) half of the packed products
-#pragma unroll
-            for (int k = 0; k < kPairs; ++k) qacc[k][0] = qacc[k][1] = make_float2(0.f, 0.f);
             bool ok = true;
             // Tail of a partial last chunk: complex64 / bfloat16 pairs that start
             // before len lie in the copied bytes (rounded up into the zeroed
@@ -1353,42 +1351,60 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
                     ok = false;
                     break;
                 }
-                M2 v[kPairs][2];
-                tile_pairs<C2, MASK>(ring + size_t(s) * P::TILE, len, v);
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[s]);
-                if (tt == 0) {
+                if constexpr (std::is_same<C2, bf2>::value) {
+                    // packed words straight from the tile; u -= h v as two
+                    // fp32x2 FMAs per value: (v.re, v.im) (-h.re, -h.re) and
+                    // the swapped pair (v.im, v.re) (h.im, -h.im), both pairs
+                    // widened from the word by a shift and a mask
+                    uint4 raw[kPairs / 2];
 #pragma unroll
-                    for (int k = 0; k < kPairs; ++k) u[k][0] = v[k][0], u[k][1] = v[k][1];
-                    continue;
-                }
-                const M2 h = hm[tt - 1];
+                    for (int w4 = 0; w4 < kPairs / 2; ++w4)
+                        raw[w4] = reinterpret_cast<const uint4*>(ring + size_t(s) * P::TILE)
+                            [threadIdx.x + kThreads * w4];
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s]);
+                    const M2 h = tt > 0 ? hm[tt - 1] : cmake<M2>(0.0, 0.0);
+                    const float2 hre = make_float2(-h.x, -h.x), him = make_float2(h.y, -h.y);
 #pragma unroll
-                for (int k = 0; k < kPairs; ++k)
+                    for (int w4 = 0; w4 < kPairs / 2; ++w4) {
+                        const unsigned wd[4] = {raw[w4].x, raw[w4].y, raw[w4].z, raw[w4].w};
 #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
-                        if constexpr (std::is_same<C2, bf2>::value) {
-                            u[k][c] = ffma2(v[k][c], make_float2(-h.x, -h.x), u[k][c]);
-                            qacc[k][c] = ffma2(v[k][c], make_float2(-h.y, h.y), qacc[k][c]);
-                        } else {
+                        for (int c = 0; c < 4; ++c) {
+                            const float lo = __uint_as_float(wd[c] << 16);
+                            const float hi = __uint_as_float(wd[c] & 0xffff0000u);
+                            M2& acc2 = u[2 * w4 + c / 2][c % 2];
+                            if (tt == 0) {
+                                acc2 = make_float2(lo, hi);
+                            } else {
+                                acc2 = ffma2(make_float2(lo, hi), hre, acc2);
+                                acc2 = ffma2(make_float2(hi, lo), him, acc2);
+                            }
+                        }
+                    }
+                } else {
+                    M2 v[kPairs][2];
+                    tile_pairs<C2, MASK>(ring + size_t(s) * P::TILE, len, v);
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s]);
+                    if (tt == 0) {
+#pragma unroll
+                        for (int k = 0; k < kPairs; ++k) u[k][0] = v[k][0], u[k][1] = v[k][1];
+                        continue;
+                    }
+                    const M2 h = hm[tt - 1];
+#pragma unroll
+                    for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                        for (int c = 0; c < 2; ++c) {
                             u[k][c].x -= h.x * v[k][c].x - h.y * v[k][c].y;
                             u[k][c].y -= h.x * v[k][c].y + h.y * v[k][c].x;
                         }
-                    }
+                }
             }
             if (!ok) {
                 failed = 1;
                 g.status[b] = ST_DEVICE_TIMEOUT;
                 break;
-            }
-            if constexpr (std::is_same<C2, bf2>::value) {
-#pragma unroll
-                for (int k = 0; k < kPairs; ++k)
-#pragma unroll
-                    for (int c = 0; c < 2; ++c) {
-                        u[k][c].x += qacc[k][c].y;
-                        u[k][c].y += qacc[k][c].x;
-                    }
             }
             C2* w = cb.V + (long long)(j + 1) * g.nv + n0;
 #pragma unroll
