@@ -59,10 +59,16 @@ def test_batch_tuner_picks_a_feasible_width(golden, tmp_path):
     w = t.tune(s.iterative_solver, s.operator, rhs)
     assert w in (1, 2, 4) and s.iterative_solver.batch_width == w
     assert set(t.last_timings) <= {1, 2, 4} and all(v > 0 for v in t.last_timings.values())
-    # cached: a second tuner reads the width without measuring
+    # the Arnoldi kernel forms were timed too and the fastest one is set
+    entry = next(iter(t.cache.values()))
+    assert set(entry["seconds_per_rhs_iteration_by_variant"]) == {"0", "1", "2"}
+    assert s.iterative_solver.kernel_variant == entry["kernel_variant"]
+    # cached: a second tuner reads the width and form without measuring
     t2 = autotune.BatchTuner(cache_path=tmp_path / "t.json")
     s.iterative_solver.batch_width = 0
+    s.iterative_solver.kernel_variant = 0
     assert t2.tune(s.iterative_solver, s.operator, rhs) == w and t2.last_timings == {}
+    assert s.iterative_solver.kernel_variant == entry["kernel_variant"]
     # solving with the tuned width still reaches the direct solution
     from tests.helpers import rel
     x = s.solve_rhs_device(rhs).cpu().numpy()
@@ -108,3 +114,28 @@ def test_mixed_apply_on_an_uneven_grid(nrhs):
         want = op.apply(x, var, N.PREC_FP64).cpu().numpy()
         for b in range(nrhs):
             assert rel(got[b], want[b]) < 2e-6
+
+
+@pytest.mark.gpu
+def test_stencil_tuner_picks_a_kernel(golden, tmp_path):
+    """StencilTuner times both complex64 stencil kernels for a batch width,
+    caches the faster one, and the operator then applies with it (same rows
+    as the FP64 operator)."""
+    import numpy as np
+    import torch
+    from tests.helpers import golden_solver, rel
+    from ultrasound_solver_b200 import _native as N
+    s = golden_solver(golden)
+    op = s.operator
+    t = autotune.StencilTuner(cache_path=tmp_path / "s.json", reps=3)
+    k = t.tune(op, 4)
+    assert k in (N.STENCIL_COEF_ROWS, N.STENCIL_RECORD_TILES) and op.stencil_kernel == k
+    assert set(t.last_timings) == {N.STENCIL_COEF_ROWS, N.STENCIL_RECORD_TILES}
+    op.stencil_kernel = N.STENCIL_AUTO
+    assert autotune.StencilTuner(cache_path=tmp_path / "s.json").tune(op, 4) == k
+    rng = np.random.default_rng(4)
+    x = torch.from_numpy(rng.standard_normal((4, op.n)) + 1j * rng.standard_normal((4, op.n))).cuda()
+    got = op.apply(x.to(torch.complex64), N.APPLY_K, N.PREC_MIXED).cpu().numpy()
+    want = op.apply(x, N.APPLY_K, N.PREC_FP64).cpu().numpy()
+    for b in range(4):
+        assert rel(got[b], want[b]) < 2e-6

@@ -121,6 +121,18 @@ template <> __device__ __forceinline__ const OpView<double>& slot_view<double>(c
 template <> __device__ __forceinline__ const OpView<float>& slot_view<float>(const SceneSlot& s) {
     return s.op32;
 }
+// CTAs of the launch that work for right-hand side b: all of them for a
+// single scene; for a multi-scene batch a share proportional to the RHS's
+// scene size (the grid is sized for the largest scene), at least one.
+template <bool MS> __device__ __forceinline__ int rhs_ctas(const GState& g, int b) {
+    if constexpr (MS) {
+        const long long c = ((long long)gridDim.x * g.slots[b].n + g.n - 1) / g.n;
+        return int(c < 1 ? 1 : c);
+    } else {
+        return int(gridDim.x);
+    }
+}
+
 
 // host-read block offsets (in doubles)
 __host__ __device__ __forceinline__ int hb_graw(int) { return 0; }
@@ -203,12 +215,12 @@ __device__ __forceinline__ bool last_block_done(unsigned* counter, int nblk) {
 
 __device__ __forceinline__ double2 ld_cg(const double2* p) { return __ldcg(p); }
 
-// Sum of the gridDim.x norm partials (slot 0) by the last CTA, in a fixed
+// Sum of the nparts norm partials (slot 0) by the last CTA, in a fixed
 // order (thread-strided, then the block tree).
-__device__ __forceinline__ double reduce_slot0(const GState& g, int b, double* sh) {
+__device__ __forceinline__ double reduce_slot0(const GState& g, int b, double* sh, int nparts) {
     double t = 0.0;
     const double2* p = g.partial + (long long)b * g.nblk * g.ps;
-    for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x)
+    for (int q = threadIdx.x; q < nparts; q += blockDim.x)
         t += ld_cg(p + (long long)q * g.ps).x;
     return block_sum(t, sh);
 }
@@ -261,13 +273,15 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
         step = sl.step;
         nchunk = sl.nchunk;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     __shared__ double sh[32];
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     C2* v0 = cb.V + (long long)cb.kc * g.nv;
     double acc = 0.0, acc_s = 0.0;
-    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += ncta) {
         const long long n0 = (long long)ch * g.chunk;
         const long long n1 = min(n0 + g.chunk, op.n);
         Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
@@ -289,14 +303,14 @@ __global__ void __launch_bounds__(256) k_residual(OpView<double> op, const doubl
     acc_s = block_sum(acc_s, sh);
     if (threadIdx.x == 0)
         g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, acc_s);
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    if (!last_block_done(&g.counter[b], ncta)) return;
     // FP64 norm of the residual (the convergence test, like the final gate)
     // and of its stored copy (the scale of the cycle's first basis vector)
-    const double t = reduce_slot0(g, b, sh);
+    const double t = reduce_slot0(g, b, sh, ncta);
     double ts = 0.0;
     {
         const double2* pp = g.partial + (long long)b * g.nblk * g.ps;
-        for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x) ts += ld_cg(pp + (long long)q * g.ps).y;
+        for (int q = threadIdx.x; q < ncta; q += blockDim.x) ts += ld_cg(pp + (long long)q * g.ps).y;
         ts = block_sum(ts, sh);
     }
     __shared__ int st_sh;
@@ -594,10 +608,9 @@ template <> struct LaneLoad<double2> {
 // Last CTA of a dots launch: sum the per-CTA partials of t = 0..j (the dots)
 // and t = j+1 (||w||^2) in a fixed order into Hessenberg column j (or the
 // projection coefficients alpha) and wnorm.
-__device__ __forceinline__ void dots_finish(GState& g, int b, int j, bool proj) {
+__device__ __forceinline__ void dots_finish(GState& g, int b, int j, bool proj, int nparts) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nw = int(blockDim.x >> 5);
-    const int nparts = int(gridDim.x);
     for (int t = warp; t <= j + 1; t += nw) {
         double re0 = 0.0, im0 = 0.0;
         const double2* pt = g.partial + (long long)b * g.nblk * g.ps + t;
@@ -645,6 +658,8 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         op = slot_view<R>(g.slots[b]);
         step = g.slots[b].step_d;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     const bool proj = mode == 1;
     if (proj) {
@@ -674,7 +689,7 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     for (int task = threadIdx.x; task < tasks_t * segs; task += NT)
         segsum[task] = make_double2(0.0, 0.0);
     const int nphase = int((N + DC - 1) / DC);
-    for (int ch = blockIdx.x; ch < nphase; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nphase; ch += ncta) {
         const long long n0 = (long long)ch * DC;
         const int len = int(min((long long)DC, N - n0));
         __syncthreads();  // the previous chunk's dots are done with ys
@@ -770,9 +785,8 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
 #pragma unroll
                     for (int c = 0; c < NL; ++c) lre += cabs2(widen<M2>(ys[NL * q + c]));
             }
-            double re = warp_sum(double(lre));
-            double im = warp_sum(double(lim));
-            if (lane == 0) segsum[task] = cadd(segsum[task], make_double2(re, im));
+            const double v = warp_sum_pair(double(lre), double(lim));
+            if ((lane & 15) == 0) reinterpret_cast<double*>(&segsum[task])[lane >> 4] += v;
         }
     }
     __syncthreads();
@@ -790,8 +804,8 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         }
         part[t] = make_double2(re, im);
     }
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    dots_finish(g, b, j, proj);
+    if (!last_block_done(&g.counter[b], ncta)) return;
+    dots_finish(g, b, j, proj, ncta);
 }
 
 // Bulk-copy form of k_dots (bfloat16 and complex64 vectors). Per chunk of DC
@@ -834,6 +848,8 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
         op = slot_view<R>(g.slots[b]);
         step = g.slots[b].step_d;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     const bool proj = mode == 1;
     if (proj) {
@@ -868,7 +884,7 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
     }
     __syncthreads();
     const int nphase = int((N + DC - 1) / DC);
-    const int nmy = nphase > int(blockIdx.x) ? (nphase - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x) : 0;
+    const int nmy = nphase > int(blockIdx.x) ? (nphase - int(blockIdx.x) + ncta - 1) / ncta : 0;
     const int tpc = j + 1;  // tiles per chunk: u_0 .. u_j
     double wn = 0.0;        // ||w||^2 of this thread's nodes
     if (warp == NWC) {
@@ -877,7 +893,7 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
             long long q = 0;
             bool ok = true;
             for (int i = 0; i < nmy && ok; ++i) {
-                const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * DC;
+                const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * DC;
                 const int len = int(min((long long)DC, N - n0));
                 const unsigned bytes = unsigned((size_t(len) * sizeof(C2) + 15) / 16 * 16);
                 for (int t = 0; t < tpc; ++t, ++q) {
@@ -901,7 +917,7 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
     } else {
         long long q = 0;
         for (int i = 0; i < nmy; ++i) {
-            const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * DC;
+            const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * DC;
             const int len = int(min((long long)DC, N - n0));
             // all consumer warps are done with ys of the previous chunk; a
             // failed wait of any warp (seen by all after the barrier) ends
@@ -967,19 +983,23 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[st]);
-                double re, im;
+                double* acc = reinterpret_cast<double*>(&wsum[warp * wst + t]);
                 if constexpr (std::is_same<C2, bf2>::value) {
-                    re = double(fre);
-                    im = double(fim);
+                    // fp32 warp sums of the (Re, Im) lane partials (8 nodes
+                    // each) with one shuffle per step: after the first
+                    // exchange the low half-warp sums Re and the high half Im;
+                    // lanes 0 and 16 add them in FP64 to the warp's row
+                    const bool hi = (lane & 16) != 0;
+                    float v = (hi ? fim : fre) + __shfl_xor_sync(0xffffffffu, hi ? fre : fim, 16);
+#pragma unroll
+                    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if ((lane & 15) == 0) acc[hi ? 1 : 0] += double(v);
                 } else {
-                    re = dre;
-                    im = dim;
-                }
-                re = warp_sum(re);
-                im = warp_sum(im);
-                if (lane == 0) {
-                    double2& acc = wsum[warp * wst + t];
-                    acc = make_double2(acc.x + re, acc.y + im);
+                    const double re = warp_sum(dre), im = warp_sum(dim);
+                    if (lane == 0) {
+                        acc[0] += re;
+                        acc[1] += im;
+                    }
                 }
             }
             if (!ok) {
@@ -1001,8 +1021,8 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
         part[t] = make_double2(re * st, im * st);
     }
     if (threadIdx.x == 0) part[j + 1] = make_double2(wn, 0.0);
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    dots_finish(g, b, j, proj);
+    if (!last_block_done(&g.counter[b], ncta)) return;
+    dots_finish(g, b, j, proj, ncta);
 }
 
 // d = a * b + c on two fp32 lanes at once (PTX fma.rn.f32x2, sm_100)
@@ -1022,9 +1042,9 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
 // harmonic Ritz step and the end-of-cycle flag.
 template <typename C2>
 __device__ __forceinline__ void orth_finish(GState& g, int b, const CycleBasis<C2>& cb, int j, int proj,
-                                         double* sh, double2* hs, double2* gsS, double* gcS) {
+                                         double* sh, double2* hs, double2* gsS, double* gcS, int nparts) {
     const int m = g.m;
-    const double beta = sqrt(reduce_slot0(g, b, sh));
+    const double beta = sqrt(reduce_slot0(g, b, sh, nparts));
     if (proj) {
         if (threadIdx.x == 0) {
             g.counter[b] = 0;
@@ -1124,6 +1144,8 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
         N = g.slots[b].n;
         nchunk = g.slots[b].nchunk;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     if (proj) {
         if (cb.kc == 0) return;
@@ -1146,7 +1168,7 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     }
     __syncthreads();  // hs, hm visible
     double acc = 0.0;
-    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += ncta) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
         C2* w = cb.V + (long long)(j + 1) * g.nv + n0;
@@ -1198,8 +1220,8 @@ __global__ void __launch_bounds__(kThreads) k_orth(S* V, long long N, GState g, 
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0)
         g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    orth_finish<C2>(g, b, cb, j, proj, sh, hs, gsS, gcS);
+    if (!last_block_done(&g.counter[b], ncta)) return;
+    orth_finish<C2>(g, b, cb, j, proj, sh, hs, gsS, gcS, ncta);
 }
 
 // Bulk-copy form of k_orth: the basis tiles reach shared memory by
@@ -1266,6 +1288,8 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
         N = g.slots[b].n;
         nchunk = g.slots[b].nchunk;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const CycleBasis<C2> cb = cycle_basis(V, g, b);
     if (proj) {
         if (cb.kc == 0) return;
@@ -1300,7 +1324,7 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
     }
     __syncthreads();  // hs, hm, barriers visible
     const int tpc = j + 2;  // tiles per chunk: w, u_0 .. u_j
-    const int nmy = nchunk > int(blockIdx.x) ? int((nchunk - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
+    const int nmy = nchunk > int(blockIdx.x) ? int((nchunk - blockIdx.x + ncta - 1) / ncta) : 0;
     double acc = 0.0;
     if (warp == kThreads / 32) {
         // producer: one elected thread issues every tile of this CTA in order
@@ -1308,7 +1332,7 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
             int q = 0;
             bool ok = true;
             for (int i = 0; i < nmy && ok; ++i) {
-                const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
+                const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * kChunk;
                 const int len = int(min((long long)kChunk, N - n0));
                 const unsigned bytes = unsigned((size_t(len) * sizeof(C2) + 15) / 16 * 16);
                 for (int tt = 0; tt < tpc; ++tt, ++q) {
@@ -1336,7 +1360,7 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
     } else {
         int q = 0;
         for (int i = 0; i < nmy; ++i) {
-            const long long n0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * kChunk;
+            const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * kChunk;
             const int len = int(min((long long)kChunk, N - n0));
             M2 u[kPairs][2];
             bool ok = true;
@@ -1361,8 +1385,6 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
                     for (int w4 = 0; w4 < kPairs / 2; ++w4)
                         raw[w4] = reinterpret_cast<const uint4*>(ring + size_t(s) * P::TILE)
                             [threadIdx.x + kThreads * w4];
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&empty[s]);
                     const M2 h = tt > 0 ? hm[tt - 1] : cmake<M2>(0.0, 0.0);
                     const float2 hre = make_float2(-h.x, -h.x), him = make_float2(h.y, -h.y);
 #pragma unroll
@@ -1384,22 +1406,25 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
                 } else {
                     M2 v[kPairs][2];
                     tile_pairs<C2, MASK>(ring + size_t(s) * P::TILE, len, v);
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&empty[s]);
                     if (tt == 0) {
 #pragma unroll
                         for (int k = 0; k < kPairs; ++k) u[k][0] = v[k][0], u[k][1] = v[k][1];
-                        continue;
+                    } else {
+                        const M2 h = hm[tt - 1];
+#pragma unroll
+                        for (int k = 0; k < kPairs; ++k)
+#pragma unroll
+                            for (int c = 0; c < 2; ++c) {
+                                u[k][c].x -= h.x * v[k][c].x - h.y * v[k][c].y;
+                                u[k][c].y -= h.x * v[k][c].y + h.y * v[k][c].x;
+                            }
                     }
-                    const M2 h = hm[tt - 1];
-#pragma unroll
-                    for (int k = 0; k < kPairs; ++k)
-#pragma unroll
-                        for (int c = 0; c < 2; ++c) {
-                            u[k][c].x -= h.x * v[k][c].x - h.y * v[k][c].y;
-                            u[k][c].y -= h.x * v[k][c].y + h.y * v[k][c].x;
-                        }
                 }
+                // the stage is released only after its values have been used
+                // (their loads have completed), so the producer's next copy
+                // into it cannot overtake a read of this warp
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[s]);
             }
             if (!ok) {
                 failed = 1;
@@ -1422,8 +1447,8 @@ __global__ void __launch_bounds__(OrthBulk<S>::THREADS) k_orth_bulk(S* V, long l
     if (failed) return;
     if (threadIdx.x == 0)
         g.partial[((long long)b * g.nblk + blockIdx.x) * g.ps] = make_double2(acc, 0.0);
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
-    orth_finish<C2>(g, b, cb, j, proj, sh, hs, gsS, gcS);
+    if (!last_block_done(&g.counter[b], ncta)) return;
+    orth_finish<C2>(g, b, cb, j, proj, sh, hs, gsS, gcS, ncta);
 }
 
 // ------------------------------------------------------------ least squares (once per cycle)
@@ -1488,6 +1513,8 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
         op = g.slots[b].op64;
         nchunk = g.slots[b].nchunk;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     extern __shared__ __align__(16) uint4 stg[];
     __shared__ double2 ys[USV_MAX_RESTART];
     __shared__ float2 yf[USV_MAX_RESTART];
@@ -1500,7 +1527,7 @@ __global__ void __launch_bounds__(kThreads) k_update(OpView<double> op, const S*
     // solution vectors: U_t (t < kc) of the cycle's pair, then Krylov slots
     const CycleBasis<C2> cb = cycle_basis(const_cast<C2*>(V), g, b);
     __syncthreads();  // ys visible
-    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += ncta) {
         const long long n0 = (long long)ch * kChunk;
         const int len = int(min((long long)kChunk, N - n0));
         double2 acc[kPairs][2];
@@ -1568,6 +1595,8 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
         N = g.slots[b].n;
         nchunk = g.slots[b].nchunk;
     }
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const CycleBasis<S> cb = cycle_basis(V, g, b);
     const int m = g.m;
     if (cb.kc != K) return;  // recycled cycles use all K vectors
@@ -1579,7 +1608,7 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
     for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) tab[q] = make_double2(0.0, 0.0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int nw = kThreads / 32;
-    for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+    for (int ch = blockIdx.x; ch < nchunk; ch += ncta) {
         for (int t0 = 0; t0 < kChunk; t0 += kBdTile) {
             const long long n0 = (long long)ch * kChunk + t0;
             const int len = int(max(0LL, min((long long)kBdTile, N - n0)));
@@ -1616,13 +1645,13 @@ __global__ void __launch_bounds__(kThreads) k_bdots(S* V, long long N, GState g)
     __syncthreads();
     double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
     for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) part[q] = tab[q];
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    if (!last_block_done(&g.counter[b], ncta)) return;
     const double* d = g.dU + ((long long)cb.pair * gridDim.y + b) * g.kr;
     double* out = g.hb + (long long)b * g.hb_len + hb_bd(m);
     for (int q = threadIdx.x; q < (m + 1) * kc; q += kThreads) {
         double re = 0.0, im = 0.0;
         const double2* pq = g.partial + (long long)b * g.nblk * g.ps + q;
-        for (int c = 0; c < int(gridDim.x); ++c) {
+        for (int c = 0; c < ncta; ++c) {
             const double2 v = ld_cg(pq + (long long)c * g.ps);
             re += v.x;
             im += v.y;
@@ -1652,6 +1681,8 @@ __global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState 
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE) return;
     if constexpr (MS) N = g.slots[b].n;
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const int* cw = g.ctl + b * kCtl;
     if (!cw[CW_COMBINE]) return;
     const int m = g.m, skc = cw[CW_SRC_KC];
@@ -1685,7 +1716,7 @@ __global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState 
             }
         }
     };
-    const long long step = (long long)gridDim.x * kThreads * NPT;
+    const long long step = (long long)ncta * kThreads * NPT;
     for (long long n0 = (long long)blockIdx.x * kThreads * NPT + threadIdx.x; n0 < N; n0 += step) {
         T au[NPT][K], ac[NPT][K];
 #pragma unroll
@@ -1734,11 +1765,11 @@ __global__ void __launch_bounds__(kThreads) k_combine(S* V, long long N, GState 
         const double t = block_sum(nrm[i], sh);
         if (threadIdx.x == 0) part[i] = make_double2(t, 0.0);
     }
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    if (!last_block_done(&g.counter[b], ncta)) return;
     for (int i = threadIdx.x; i < K; i += kThreads) {
         double t = 0.0;
         const double2* pq = g.partial + (long long)b * g.nblk * g.ps + i;
-        for (int c = 0; c < int(gridDim.x); ++c) t += ld_cg(pq + (long long)c * g.ps).x;
+        for (int c = 0; c < ncta; ++c) t += ld_cg(pq + (long long)c * g.ps).x;
         g.dU[((long long)cw[CW_DST] * gridDim.y + b) * K + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
     }
     if (threadIdx.x == 0) g.counter[b] = 0;
@@ -1767,6 +1798,7 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], unsigned a0, unsigned a1
 __device__ __forceinline__ unsigned bf_pack(__nv_bfloat16 lo, __nv_bfloat16 hi) {
     return unsigned(__bfloat16_as_ushort(lo)) | (unsigned(__bfloat16_as_ushort(hi)) << 16);
 }
+constexpr int kCombineGroup = 6;  // k-blocks of 8 input rows loaded per batch
 static size_t combine_mma_smem(int k, int m) {
     return sizeof(uint2) * size_t((k + m + 1 + 7) / 8) * k * 32;
 }
@@ -1775,6 +1807,8 @@ __global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, G
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE) return;
     if constexpr (MS) N = g.slots[b].n;
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const int* cw = g.ctl + b * kCtl;
     if (!cw[CW_COMBINE]) return;
     const int m = g.m, skc = cw[CW_SRC_KC];
@@ -1821,26 +1855,38 @@ __global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, G
 #pragma unroll
     for (int i = 0; i < K; ++i) nrm[i] = 0.f;
     const long long nblk16 = (N + 15) / 16;
-    const long long wstride = (long long)gridDim.x * (kThreads / 32);
+    const long long wstride = (long long)ncta * (kThreads / 32);
     for (long long blk = (long long)blockIdx.x * (kThreads / 32) + warp; blk < nblk16; blk += wstride) {
         const long long n0 = blk * 16 + g8, n1 = n0 + 8;
         const long long l0 = n0 < N ? n0 : N - 1, l1 = n1 < N ? n1 : N - 1;
         float acc[K][4];
 #pragma unroll
         for (int nt = 0; nt < K; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-#pragma unroll 2
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int ra = 8 * kb + c4, rb = ra + 4;
-            const unsigned* pa = row(ra);
-            const unsigned* pb = row(rb);
-            unsigned a0 = __ldg(pa + l0), a1 = __ldg(pa + l1), a2 = __ldg(pb + l0), a3 = __ldg(pb + l1);
-            if (ra >= rows) a0 = a1 = 0u;
-            if (rb >= rows) a2 = a3 = 0u;
-            const uint2* bq = bfr + (size_t)kb * K * 32 + lane;
+        // the A words of kCombineGroup k-blocks are loaded before their MMAs
+        // (24 loads in flight per lane instead of 4)
+        for (int kb0 = 0; kb0 < nkb; kb0 += kCombineGroup) {
+            unsigned a[kCombineGroup][4];
 #pragma unroll
-            for (int nt = 0; nt < K; ++nt) {
-                const uint2 bb = bq[nt * 32];
-                mma_bf16(acc[nt], a0, a1, a2, a3, bb.x, bb.y);
+            for (int u = 0; u < kCombineGroup; ++u) {
+                const int ra = 8 * (kb0 + u) + c4, rb = ra + 4;
+                const unsigned* pa = row(ra);
+                const unsigned* pb = row(rb);
+                a[u][0] = __ldg(pa + l0);
+                a[u][1] = __ldg(pa + l1);
+                a[u][2] = __ldg(pb + l0);
+                a[u][3] = __ldg(pb + l1);
+                if (ra >= rows) a[u][0] = a[u][1] = 0u;
+                if (rb >= rows) a[u][2] = a[u][3] = 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < kCombineGroup; ++u) {
+                if (kb0 + u >= nkb) break;
+                const uint2* bq = bfr + (size_t)(kb0 + u) * K * 32 + lane;
+#pragma unroll
+                for (int nt = 0; nt < K; ++nt) {
+                    const uint2 bb = bq[nt * 32];
+                    mma_bf16(acc[nt], a[u][0], a[u][1], a[u][2], a[u][3], bb.x, bb.y);
+                }
             }
         }
         // lanes c and c^1 hold the hi and lo parts of one output: add them;
@@ -1883,11 +1929,11 @@ __global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, G
         for (int w = 0; w < kThreads / 32; ++w) t += sh[w][o];
         part[o] = make_double2(t, 0.0);
     }
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    if (!last_block_done(&g.counter[b], ncta)) return;
     for (int i = threadIdx.x; i < K; i += kThreads) {
         double t = 0.0;
         const double2* pq = g.partial + (long long)b * g.nblk * g.ps + i;
-        for (int c = 0; c < int(gridDim.x); ++c) t += ld_cg(pq + (long long)c * g.ps).x;
+        for (int c = 0; c < ncta; ++c) t += ld_cg(pq + (long long)c * g.ps).x;
         g.dU[((long long)cw[CW_DST] * gridDim.y + b) * K + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
     }
     if (threadIdx.x == 0) g.counter[b] = 0;
@@ -1909,6 +1955,8 @@ __global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GSt
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || !g.ended[b]) return;
     if constexpr (MS) N = g.slots[b].n;
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     const CycleBasis<bf2> cb = cycle_basis(V, g, b);
     const int m = g.m;
     if (cb.kc != K) return;  // recycled cycles use all K vectors
@@ -1920,7 +1968,7 @@ __global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GSt
     const int g8 = lane >> 2, c4 = lane & 3;
     constexpr int nw = kThreads / 32;
 
-    const long long W = (long long)gridDim.x * nw, wg = (long long)blockIdx.x * nw + warp;
+    const long long W = (long long)ncta * nw, wg = (long long)blockIdx.x * nw + warp;
     const int rt = int(wg % RT);
     const long long wstride = W / RT;
     const int sa = 16 * rt + g8, sb = sa + 8;
@@ -1947,25 +1995,41 @@ __global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GSt
             float d[NT][4];
 #pragma unroll
             for (int nt = 0; nt < NT; ++nt) d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
-            for (int r = 0; r < 16 && blk < nb16; ++r, blk += wstride) {
-                const long long uq = 4 * blk + c4;
-                const long long uc = uq < lastu ? uq : lastu;
-                uint4 va = __ldg(pa + uc), vb = __ldg(pb + uc);
-                if (!(sa <= m && uq <= lastu)) va = zero;
-                if (!(sb <= m && uq <= lastu)) vb = zero;
+            // two blocks of 16 nodes per batch: their 2 (2 + NT) 16-byte loads
+            // are issued before the MMAs of either
+            for (int r = 0; r < 16 && blk < nb16; r += 2) {
+                uint4 va[2], vb[2], w[2][NT];
 #pragma unroll
-                for (int nt = 0; nt < NT; ++nt) {
-                    uint4 w = __ldg(pu[nt] + uc);
-                    if (!(4 * nt + g8 / 2 < K && uq <= lastu)) w = zero;
-                    if (g8 & 1) {
-                        w.x = (w.x >> 16) | ((w.x << 16) ^ 0x80000000u);
-                        w.y = (w.y >> 16) | ((w.y << 16) ^ 0x80000000u);
-                        w.z = (w.z >> 16) | ((w.z << 16) ^ 0x80000000u);
-                        w.w = (w.w >> 16) | ((w.w << 16) ^ 0x80000000u);
+                for (int u = 0; u < 2; ++u) {
+                    const long long bu = blk + u * wstride;
+                    const long long uq = 4 * bu + c4;
+                    const bool in = bu < nb16 && uq <= lastu;
+                    const long long uc = uq < lastu ? uq : lastu;
+                    va[u] = __ldg(pa + uc);
+                    vb[u] = __ldg(pb + uc);
+                    if (!(sa <= m && in)) va[u] = zero;
+                    if (!(sb <= m && in)) vb[u] = zero;
+#pragma unroll
+                    for (int nt = 0; nt < NT; ++nt) {
+                        w[u][nt] = __ldg(pu[nt] + uc);
+                        if (!(4 * nt + g8 / 2 < K && in)) w[u][nt] = zero;
                     }
-                    mma_bf16(d[nt], va.x, vb.x, va.y, vb.y, w.x, w.y);
-                    mma_bf16(d[nt], va.z, vb.z, va.w, vb.w, w.z, w.w);
                 }
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+#pragma unroll
+                    for (int nt = 0; nt < NT; ++nt) {
+                        uint4 ww = w[u][nt];
+                        if (g8 & 1) {
+                            ww.x = (ww.x >> 16) | ((ww.x << 16) ^ 0x80000000u);
+                            ww.y = (ww.y >> 16) | ((ww.y << 16) ^ 0x80000000u);
+                            ww.z = (ww.z >> 16) | ((ww.z << 16) ^ 0x80000000u);
+                            ww.w = (ww.w >> 16) | ((ww.w << 16) ^ 0x80000000u);
+                        }
+                        mma_bf16(d[nt], va[u].x, vb[u].x, va[u].y, vb[u].y, ww.x, ww.y);
+                        mma_bf16(d[nt], va[u].z, vb[u].z, va[u].w, vb[u].w, ww.z, ww.w);
+                    }
+                blk += 2 * wstride;
             }
 #pragma unroll
             for (int nt = 0; nt < NT; ++nt) {
@@ -1998,13 +2062,13 @@ __global__ void __launch_bounds__(kThreads) k_bdots_mma(bf2* V, long long N, GSt
     __syncthreads();
     double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
     for (int q = threadIdx.x; q < (m + 1) * K; q += kThreads) part[q] = tab[q];
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    if (!last_block_done(&g.counter[b], ncta)) return;
     const double* dd = g.dU + ((long long)cb.pair * gridDim.y + b) * g.kr;
     double* out = g.hb + (long long)b * g.hb_len + hb_bd(m);
     for (int q = threadIdx.x; q < (m + 1) * K; q += kThreads) {
         double re = 0.0, im = 0.0;
         const double2* pq = g.partial + (long long)b * g.nblk * g.ps + q;
-        for (int c = 0; c < int(gridDim.x); ++c) {
+        for (int c = 0; c < ncta; ++c) {
             const double2 v = ld_cg(pq + (long long)c * g.ps);
             re += v.x;
             im += v.y;
@@ -2025,12 +2089,14 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
                                                const double2* x, long long ld, GState g) {
     const int b = blockIdx.y;
     if constexpr (MS) op = g.slots[b].op64;
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
     __shared__ double sh[32];
     const double2* rb = rhs + b * ld;
     const double2* xb = x + b * ld;
     double s2 = 0.0, b2 = 0.0, bwd = 0.0, bad = 0.0;
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < op.n;
-         n += (long long)gridDim.x * blockDim.x) {
+         n += (long long)ncta * blockDim.x) {
         const Node p = decode(n, op.nx, op.ny);
         const double2 ax = a_row<ADJ ? USV_APPLY_AH : USV_APPLY_A>(op, xb, n, p);
         const double2 den = a_row<ADJ ? USV_APPLY_ABS_AH : USV_APPLY_ABS_A>(op, xb, n, p);
@@ -2052,9 +2118,9 @@ __global__ void __launch_bounds__(256) k_gates(OpView<double> op, const double2*
         part[0] = make_double2(s2, b2);
         part[1] = make_double2(bwd, bad);
     }
-    if (!last_block_done(&g.counter[b], gridDim.x)) return;
+    if (!last_block_done(&g.counter[b], ncta)) return;
     double ts = 0, tb = 0, tw = 0, tbad = 0;
-    for (int q = threadIdx.x; q < int(gridDim.x); q += blockDim.x) {
+    for (int q = threadIdx.x; q < ncta; q += blockDim.x) {
         const double2* pq = g.partial + ((long long)b * g.nblk + q) * g.ps;
         const double2 p0 = ld_cg(pq), p1 = ld_cg(pq + 1);
         ts += p0.x;
@@ -2238,7 +2304,16 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     auto grid_for = [&](const void* fn, int threads, size_t smem, dim3& grid) -> int {
         int per_sm = 0;
         USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+        // one wave of resident CTAs shared by the right-hand sides; for a
+        // multi-scene batch the grid is sized so that the per-RHS shares
+        // (proportional to the scene sizes, rhs_ctas) add up to that wave
         long long x = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1) / B;
+        if constexpr (MS) {
+            double total = 0.0;
+            for (const SceneSlot& sl : *slots) total += double(sl.n);
+            x = (long long)(double((per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1)) *
+                            double(g.n) / total);
+        }
         if (p.max_ctas > 0 && x > p.max_ctas) x = p.max_ctas;
         x = x < 1 ? 1 : (x > g.nchunk ? g.nchunk : x);
         grid = dim3(unsigned(x), unsigned(B));

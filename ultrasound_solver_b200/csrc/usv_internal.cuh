@@ -575,6 +575,16 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// Warp sums of two values with one shuffle per step: after the first exchange
+// the low half-warp carries a, the high half b; returns a's sum in lanes
+// 0..15 and b's sum in lanes 16..31 (lane 0 and lane 16 hold the results).
+__device__ __forceinline__ double warp_sum_pair(double a, double b) {
+    const bool hi = (threadIdx.x & 16) != 0;
+    double v = (hi ? b : a) + __shfl_xor_sync(0xffffffffu, hi ? a : b, 16);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
