@@ -2272,6 +2272,7 @@ static bool recycle_coefficients(int m, int k, const double* hb, std::vector<dou
     return finite;
 }
 
+constexpr double kSceneWaves = 4.0;  // multi-scene grids: waves of CTA shares
 template <typename R, typename S, bool ADJ, bool MS = false>
 static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_params& p,
                      const double2* rhs, double2* x, int B, long long ld, char* ws,
@@ -2304,14 +2305,16 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     auto grid_for = [&](const void* fn, int threads, size_t smem, dim3& grid) -> int {
         int per_sm = 0;
         USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
-        // one wave of resident CTAs shared by the right-hand sides; for a
-        // multi-scene batch the grid is sized so that the per-RHS shares
-        // (proportional to the scene sizes, rhs_ctas) add up to that wave
+        // one wave of resident CTAs shared by the right-hand sides. For a
+        // multi-scene batch the per-RHS shares are proportional to the scene
+        // sizes (rhs_ctas) and add up to kSceneWaves waves while every RHS is
+        // active: when the small scenes have converged, the large ones still
+        // fill the GPU (CTAs of finished right-hand sides return at once)
         long long x = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1) / B;
         if constexpr (MS) {
             double total = 0.0;
             for (const SceneSlot& sl : *slots) total += double(sl.n);
-            x = (long long)(double((per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1)) *
+            x = (long long)(kSceneWaves * double((per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1)) *
                             double(g.n) / total);
         }
         if (p.max_ctas > 0 && x > p.max_ctas) x = p.max_ctas;
