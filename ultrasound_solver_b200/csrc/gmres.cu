@@ -808,49 +808,41 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     dots_finish(g, b, j, proj, ncta);
 }
 
-// Bulk-copy form of k_dots (bfloat16 and complex64 vectors). Per chunk of DC
-// nodes the consumer warps first form w = sigma_j K u_j (stencil, into shared
-// memory and the basis) while a producer warp already streams the chunk tiles
-// of u_0 .. u_j into a ring of shared-memory stages (cp.async.bulk completed
-// on full / empty mbarriers, kDotsStages - 1 tiles ahead). Every consumer
-// warp then owns one 1/16 slice of the chunk and forms its partial
-// <sigma_t u_t, w> for every tile t, reduced over the warp and added in FP64
-// to its own row of per-warp sums (no load imbalance between the dot tasks);
-// ||w||^2 is summed while w is formed. All waits are bounded
-// (ST_DEVICE_TIMEOUT, then a bounded drain of the copies in flight).
-template <typename S> struct DotsBulk {
-    static constexpr int DC = std::is_same<S, bf2>::value ? 2 * kChunk : kChunk;  // nodes per chunk
-    static constexpr int TILE = DC * int(sizeof(S));
-    static constexpr int STAGES = 4;
-    static constexpr int NWC = kDotsThreads / 32;                                // consumer warps
-    using YS = typename std::conditional<std::is_same<S, float2>::value, double2, S>::type;
-    static constexpr int THREADS = kDotsThreads + 32;
-    // ring, w of the chunk, per-warp sums of the m + 1 dots, barriers
+// Bulk-copy form of k_dots for bfloat16 vectors (USV_GMRES_DOTS_BULK), laid
+// out like k_orth_bulk: a CTA works on 2048-node chunks; each of the 256
+// consumer threads first forms w = sigma_j K u_j at its 8 nodes (stencil,
+// stored into the basis and kept in registers as packed bf16 words) while a
+// producer warp streams the chunk tiles of u_0 .. u_j through a 4-stage ring
+// of full / empty mbarriers (cp.async.bulk). Per tile every thread adds the
+// bf16 x bf16 products of its 8 nodes (fp32) to a partial sum in shared
+// memory that it shares with its neighbour lane (one shuffle), so no warp
+// reduction runs per tile; after the last chunk the CTA sums the partials of
+// each t in FP64 in a fixed order. ||w||^2 is summed while w is formed. All
+// waits are bounded (ST_DEVICE_TIMEOUT, then a bounded drain of the copies
+// in flight).
+struct DotsBulk {
+    static constexpr int LOG_STAGES = 2;
+    static constexpr int STAGES = 1 << LOG_STAGES;
+    static constexpr int TILE = kChunk * int(sizeof(bf2));  // bytes per chunk tile
+    static constexpr int THREADS = kThreads + 32;           // + the producer warp
+    static constexpr int SLOTS = kThreads / 2;              // partial sums per t
+    // ring, the fp32 partials of the m + 1 dots, barriers
     static size_t smem(int m) {
-        return size_t(STAGES) * TILE + size_t(DC) * sizeof(YS) +
-               size_t(NWC) * size_t(m + 1) * sizeof(double2) + 2 * STAGES * sizeof(unsigned long long);
+        return size_t(STAGES) * TILE + size_t(m + 1) * SLOTS * sizeof(float2) +
+               2 * STAGES * sizeof(unsigned long long);
     }
 };
 
-template <typename R, typename S, bool ADJ, bool MS = false>
-__global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R> op, S* V, GState g,
-                                                                      int j, Step step, int mode) {
-    using C2 = S;
-    using P = DotsBulk<S>;
-    using YS = typename P::YS;
-    constexpr int DC = P::DC, NWC = P::NWC;
-    constexpr int NL = LaneLoad<C2>::NL;        // nodes per 16-byte group
-    constexpr int GPW = DC / NL / NWC / 32;     // groups per lane and tile
-    static_assert(GPW >= 1 && DC % (NL * NWC * 32) == 0, "chunk / warp slicing");
+template <typename R, bool ADJ, bool MS = false>
+__global__ void __launch_bounds__(DotsBulk::THREADS) k_dots_bulk(OpView<R> op, bf2* V, GState g,
+                                                                 int j, Step step, int mode) {
+    using P = DotsBulk;
     const int b = blockIdx.y;
     if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
-    if constexpr (MS) {
-        op = slot_view<R>(g.slots[b]);
-        step = g.slots[b].step_d;
-    }
+    if constexpr (MS) op = slot_view<R>(g.slots[b]);
     const int ncta = rhs_ctas<MS>(g, b);
     if (int(blockIdx.x) >= ncta) return;
-    const CycleBasis<C2> cb = cycle_basis(V, g, b);
+    const CycleBasis<bf2> cb = cycle_basis(V, g, b);
     const bool proj = mode == 1;
     if (proj) {
         if (cb.kc == 0) return;
@@ -860,49 +852,47 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
     }
     extern __shared__ __align__(128) char dyn[];
     char* ring = dyn;
-    YS* ys = reinterpret_cast<YS*>(dyn + size_t(P::STAGES) * P::TILE);
-    const int wst = g.m + 1;  // row stride of the per-warp sums
-    double2* wsum = reinterpret_cast<double2*>(reinterpret_cast<char*>(ys) + size_t(DC) * sizeof(YS));
+    float2* psum = reinterpret_cast<float2*>(dyn + size_t(P::STAGES) * P::TILE);  // [m+1][SLOTS]
     unsigned long long* full = reinterpret_cast<unsigned long long*>(
-        reinterpret_cast<char*>(wsum) + size_t(NWC) * wst * sizeof(double2));
+        reinterpret_cast<char*>(psum) + size_t(g.m + 1) * P::SLOTS * sizeof(float2));
     unsigned long long* empty = full + P::STAGES;
     __shared__ double sh[32];
     __shared__ int failed;
     const long long N = op.n;
-    const C2* uj = cb.V + (long long)j * g.nv;
-    C2* w = cb.V + (long long)(j + 1) * g.nv;
+    const bf2* uj = cb.V + (long long)j * g.nv;
+    bf2* w = cb.V + (long long)(j + 1) * g.nv;
     const R sj = R(g.sigma[b * (g.m + 1) + j]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < NWC * wst; i += blockDim.x) wsum[i] = make_double2(0.0, 0.0);
+    for (int i = threadIdx.x; i < (j + 1) * P::SLOTS; i += blockDim.x) psum[i] = make_float2(0.f, 0.f);
     if (threadIdx.x == 0) {
         failed = 0;
         for (int st = 0; st < P::STAGES; ++st) {
             mbar_init(&full[st], 1);
-            mbar_init(&empty[st], NWC);
+            mbar_init(&empty[st], kThreads / 32);
         }
         mbar_fence_init();
     }
     __syncthreads();
-    const int nphase = int((N + DC - 1) / DC);
-    const int nmy = nphase > int(blockIdx.x) ? (nphase - int(blockIdx.x) + ncta - 1) / ncta : 0;
+    const int nchunk = int((N + kChunk - 1) / kChunk);
+    const int nmy = nchunk > int(blockIdx.x) ? (nchunk - int(blockIdx.x) + ncta - 1) / ncta : 0;
     const int tpc = j + 1;  // tiles per chunk: u_0 .. u_j
     double wn = 0.0;        // ||w||^2 of this thread's nodes
-    if (warp == NWC) {
-        // producer warp: one elected thread issues the tiles of every chunk
+    if (warp == kThreads / 32) {
+        // producer: one elected thread issues the tiles of every chunk in order
         if (lane == 0) {
-            long long q = 0;
+            int q = 0;
             bool ok = true;
             for (int i = 0; i < nmy && ok; ++i) {
-                const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * DC;
-                const int len = int(min((long long)DC, N - n0));
-                const unsigned bytes = unsigned((size_t(len) * sizeof(C2) + 15) / 16 * 16);
+                const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * kChunk;
+                const int len = int(min((long long)kChunk, N - n0));
+                const unsigned bytes = unsigned((size_t(len) * sizeof(bf2) + 15) / 16 * 16);
                 for (int t = 0; t < tpc; ++t, ++q) {
-                    const int st = int(q % P::STAGES);
-                    if (!mbar_wait(&empty[st], unsigned((q / P::STAGES) & 1) ^ 1u)) {
+                    const int st = q & (P::STAGES - 1);
+                    if (!mbar_wait(&empty[st], (unsigned(q >> P::LOG_STAGES) & 1u) ^ 1u)) {
                         ok = false;
                         break;
                     }
-                    const C2* src = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
+                    const bf2* src = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
                     mbar_expect_tx(&full[st], bytes);
                     bulk_g2s(ring + size_t(st) * P::TILE, src, bytes, &full[st]);
                 }
@@ -911,114 +901,104 @@ __global__ void __launch_bounds__(DotsBulk<S>::THREADS, 2) k_dots_bulk(OpView<R>
                 failed = 1;
                 g.status[b] = ST_DEVICE_TIMEOUT;
             }
-            for (long long r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
-                mbar_wait(&full[r % P::STAGES], unsigned((r / P::STAGES) & 1));
+            for (int r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
+                mbar_wait(&full[r & (P::STAGES - 1)], unsigned(r >> P::LOG_STAGES) & 1u);
         }
     } else {
-        long long q = 0;
-        for (int i = 0; i < nmy; ++i) {
-            const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * DC;
-            const int len = int(min((long long)DC, N - n0));
-            // all consumer warps are done with ys of the previous chunk; a
-            // failed wait of any warp (seen by all after the barrier) ends
-            // the loop for every consumer at the same point
-            asm volatile("bar.sync 1, %0;" ::"n"(kDotsThreads) : "memory");
-            if (failed) break;
-            if (mode == 0) {
-                Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-                constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
-#pragma unroll(kStencilUnroll)
-                for (int e = threadIdx.x; e < DC; e += kDotsThreads) {
-                    C2 y = from_d<C2>(make_double2(0.0, 0.0));
-                    if (e < len) {
-                        const long long n = n0 + e;
-                        y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
-                        w[n] = y;
-                        wn += double(cabs2(to_d(y)));
+        int q = 0;
+        bool ok = true;
+        for (int i = 0; i < nmy && ok; ++i) {
+            const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * kChunk;
+            const int len = int(min((long long)kChunk, N - n0));
+            // w at this thread's nodes: two units of 4 consecutive nodes
+            unsigned wv[8];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int e0 = 4 * (threadIdx.x + kThreads * u);
+                unsigned wd[4];
+                if (mode == 0) {
+                    Node p = decode(n0 + e0, op.nx, op.ny);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        bf2 y = from_d<bf2>(make_double2(0.0, 0.0));
+                        if (e0 + c < len)
+                            y = narrow<bf2>(cscale(k_row<R, ADJ, bf2>(op, uj, n0 + e0 + c, p), sj));
+                        wd[c] = *reinterpret_cast<const unsigned*>(&y);
+                        if (++p.i == op.nx) {
+                            p.i = 0;
+                            if (++p.j == op.ny) {
+                                p.j = 0;
+                                ++p.k;
+                            }
+                        }
                     }
-                    ys[e] = as_ys<YS>(y);
-                    advance(p, step, op.nx, op.ny);
+                    if (e0 + 3 < len) {
+                        *reinterpret_cast<uint4*>(w + n0 + e0) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+                    } else {
+                        for (int c = 0; c < 4 && e0 + c < len; ++c)
+                            reinterpret_cast<unsigned*>(w + n0 + e0)[c] = wd[c];
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        wd[c] = e0 + c < len ? reinterpret_cast<const unsigned*>(w + n0 + e0)[c] : 0u;
                 }
-            } else {
-                for (int e = threadIdx.x; e < DC; e += kDotsThreads) {
-                    const C2 y = e < len ? w[n0 + e] : from_d<C2>(make_double2(0.0, 0.0));
-                    wn += double(cabs2(to_d(y)));
-                    ys[e] = as_ys<YS>(y);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    wv[4 * u + c] = wd[c];
+                    const float2 f = bf2_to_f2(*reinterpret_cast<const bf2*>(&wd[c]));
+                    wn += double(f.x * f.x + f.y * f.y);
                 }
             }
-            asm volatile("bar.sync 1, %0;" ::"n"(kDotsThreads) : "memory");
-            const int nvalid = (len + NL - 1) / NL;  // groups holding a node of the chunk
-            bool ok = true;
+            // dots of w with the chunk tiles of u_0 .. u_j (units starting
+            // past len read stale bytes but meet w = 0 there)
             for (int t = 0; t < tpc; ++t, ++q) {
-                const int st = int(q % P::STAGES);
-                if (!mbar_wait(&full[st], unsigned((q / P::STAGES) & 1))) {
+                const int st = q & (P::STAGES - 1);
+                if (!mbar_wait(&full[st], unsigned(q >> P::LOG_STAGES) & 1u)) {
                     ok = false;
                     break;
                 }
-                const char* tile = ring + size_t(st) * P::TILE;
-                float fre = 0.f, fim = 0.f;
-                double dre = 0.0, dim = 0.0;
-#pragma unroll
-                for (int u = 0; u < GPW; ++u) {
-                    const int qg = (warp * GPW + u) * 32 + lane;  // 16-byte group of the tile
-                    if (qg >= nvalid) continue;
-                    if constexpr (std::is_same<C2, bf2>::value) {
-                        const uint4 a = reinterpret_cast<const uint4*>(tile)[qg];
-                        const uint4 y = reinterpret_cast<const uint4*>(ys)[qg];
-                        float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
-                        bf_mac(rr, ii, ri, ir, a.x, y.x);
-                        bf_mac(rr, ii, ri, ir, a.y, y.y);
-                        bf_mac(rr, ii, ri, ir, a.z, y.z);
-                        bf_mac(rr, ii, ri, ir, a.w, y.w);
-                        fre += rr + ii;
-                        fim += ri - ir;
-                    } else {
-                        const float4 a = reinterpret_cast<const float4*>(tile)[qg];
-                        const double2 y0 = ys[2 * qg], y1 = ys[2 * qg + 1];
-                        dre = fma(double(a.x), y0.x, fma(double(a.y), y0.y, dre));
-                        dim = fma(double(a.x), y0.y, fma(-double(a.y), y0.x, dim));
-                        dre = fma(double(a.z), y1.x, fma(double(a.w), y1.y, dre));
-                        dim = fma(double(a.z), y1.y, fma(-double(a.w), y1.x, dim));
-                    }
-                }
+                const uint4* tile = reinterpret_cast<const uint4*>(ring + size_t(st) * P::TILE);
+                const uint4 a0 = tile[threadIdx.x], a1 = tile[threadIdx.x + kThreads];
+                float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
+                bf_mac(rr, ii, ri, ir, a0.x, wv[0]);
+                bf_mac(rr, ii, ri, ir, a0.y, wv[1]);
+                bf_mac(rr, ii, ri, ir, a0.z, wv[2]);
+                bf_mac(rr, ii, ri, ir, a0.w, wv[3]);
+                bf_mac(rr, ii, ri, ir, a1.x, wv[4]);
+                bf_mac(rr, ii, ri, ir, a1.y, wv[5]);
+                bf_mac(rr, ii, ri, ir, a1.z, wv[6]);
+                bf_mac(rr, ii, ri, ir, a1.w, wv[7]);
+                // the stage is released after its values have been used
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[st]);
-                double* acc = reinterpret_cast<double*>(&wsum[warp * wst + t]);
-                if constexpr (std::is_same<C2, bf2>::value) {
-                    // fp32 warp sums of the (Re, Im) lane partials (8 nodes
-                    // each) with one shuffle per step: after the first
-                    // exchange the low half-warp sums Re and the high half Im;
-                    // lanes 0 and 16 add them in FP64 to the warp's row
-                    const bool hi = (lane & 16) != 0;
-                    float v = (hi ? fim : fre) + __shfl_xor_sync(0xffffffffu, hi ? fre : fim, 16);
-#pragma unroll
-                    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if ((lane & 15) == 0) acc[hi ? 1 : 0] += double(v);
-                } else {
-                    const double re = warp_sum(dre), im = warp_sum(dim);
-                    if (lane == 0) {
-                        acc[0] += re;
-                        acc[1] += im;
-                    }
+                float re = rr + ii, im = ri - ir;
+                re += __shfl_xor_sync(0xffffffffu, re, 1);
+                im += __shfl_xor_sync(0xffffffffu, im, 1);
+                if ((lane & 1) == 0) {
+                    float2& ps = psum[t * P::SLOTS + (threadIdx.x >> 1)];
+                    ps = make_float2(ps.x + re, ps.y + im);
                 }
             }
-            if (!ok) {
-                failed = 1;
-                g.status[b] = ST_DEVICE_TIMEOUT;
-            }
+        }
+        if (!ok) {
+            failed = 1;
+            g.status[b] = ST_DEVICE_TIMEOUT;
         }
     }
-    wn = block_sum(wn, sh);
+    wn = block_sum(wn, sh);  // (its barriers also make every partial visible)
     if (failed) return;
     double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
-    for (int t = threadIdx.x; t <= j; t += blockDim.x) {
+    for (int t = warp; t <= j; t += int(blockDim.x >> 5)) {
         double re = 0.0, im = 0.0;
-        for (int ww = 0; ww < NWC; ++ww) {
-            re += wsum[ww * wst + t].x;
-            im += wsum[ww * wst + t].y;
+        for (int sl = lane; sl < P::SLOTS; sl += 32) {
+            const float2 v = psum[t * P::SLOTS + sl];
+            re += double(v.x);
+            im += double(v.y);
         }
-        const double st = g.sigma[b * (g.m + 1) + t];
-        part[t] = make_double2(re * st, im * st);
+        const double v = warp_sum_pair(re, im);
+        if ((lane & 15) == 0)
+            reinterpret_cast<double*>(&part[t])[lane >> 4] = v * g.sigma[b * (g.m + 1) + t];
     }
     if (threadIdx.x == 0) part[j + 1] = make_double2(wn, 0.0);
     if (!last_block_done(&g.counter[b], ncta)) return;
@@ -2333,11 +2313,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     const void* fn_dots = nullptr;
     int dots_threads = kDotsThreads;
     size_t dots_smem = 0;
-    if constexpr (!std::is_same<S, double2>::value) {
-        if (dots_bulk) {
-            fn_dots = (const void*)k_dots_bulk<R, S, ADJ, MS>;
-            dots_threads = DotsBulk<S>::THREADS;
-            dots_smem = DotsBulk<S>::smem(g.m);
+    if constexpr (std::is_same<S, bf2>::value) {
+        if (dots_bulk && DotsBulk::smem(g.m) <= 100 * 1024) {
+            fn_dots = (const void*)k_dots_bulk<R, ADJ, MS>;
+            dots_threads = DotsBulk::THREADS;
+            dots_smem = DotsBulk::smem(g.m);
         }
     }
     if (!fn_dots) fn_dots = (const void*)k_dots<R, S, ADJ, kDotsThreads, MS>;
