@@ -277,6 +277,7 @@ def run_ours(args):
     prof_tot = {}
     launches = 0
     iterations = []
+    cycles = []
     with ClockSampler(local) as clocks:
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
@@ -284,6 +285,7 @@ def run_ours(args):
         for _ in range(args.steps):
             x_mixed = solve(args.precision, profile=True)
             iterations.append(it.last_iterations)
+            cycles.append(max(st["cycles"] for st in it.last_stats))
             for name, d in it.last_profile.items():
                 agg = prof_tot.setdefault(name, dict(launches=0, ms=0.0, bytes=0.0))
                 for k in agg:
@@ -309,6 +311,14 @@ def run_ours(args):
            "backward_error": stats["backward_error"]}
     out["clocks"] = clocks.summary()
     out["gpu_launches"] = launches
+    # time between the measured kernel intervals: one graph launch and one
+    # status read-back per restart cycle (the cycles are not one persistent
+    # launch), plus the final gates and the stats read
+    kernel_ms = sum(v["ms"] for v in prof_tot.values())
+    out["cycle_gaps"] = {"ms_per_step": (ms_local - kernel_ms) / args.steps,
+                         "fraction_of_step": (ms_local - kernel_ms) / ms_local,
+                         "restart_cycles_per_step": statistics.mean(cycles),
+                         "us_per_cycle": 1000.0 * (ms_local - kernel_ms) / max(sum(cycles), 1)}
 
     # roofline of the dominant kernel family (live CUDA-event timing)
     peak, peak_kind = measured_peak()

@@ -950,8 +950,12 @@ __global__ void __launch_bounds__(DotsBulk::THREADS) k_dots_bulk(OpView<R> op, b
                     wn += double(f.x * f.x + f.y * f.y);
                 }
             }
-            // dots of w with the chunk tiles of u_0 .. u_j (units starting
-            // past len read stale bytes but meet w = 0 there)
+            // dots of w with the chunk tiles of u_0 .. u_j; a unit that starts
+            // past len holds stale (possibly never written) shared memory, so
+            // it is replaced by zeros (a unit that starts before len was
+            // copied, rounded up into the zeroed padding of the vector)
+            const bool in0 = 4 * int(threadIdx.x) < len, in1 = 4 * int(threadIdx.x + kThreads) < len;
+            const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
             for (int t = 0; t < tpc; ++t, ++q) {
                 const int st = q & (P::STAGES - 1);
                 if (!mbar_wait(&full[st], unsigned(q >> P::LOG_STAGES) & 1u)) {
@@ -959,7 +963,8 @@ __global__ void __launch_bounds__(DotsBulk::THREADS) k_dots_bulk(OpView<R> op, b
                     break;
                 }
                 const uint4* tile = reinterpret_cast<const uint4*>(ring + size_t(st) * P::TILE);
-                const uint4 a0 = tile[threadIdx.x], a1 = tile[threadIdx.x + kThreads];
+                const uint4 a0 = in0 ? tile[threadIdx.x] : zero4;
+                const uint4 a1 = in1 ? tile[threadIdx.x + kThreads] : zero4;
                 float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
                 bf_mac(rr, ii, ri, ir, a0.x, wv[0]);
                 bf_mac(rr, ii, ri, ir, a0.y, wv[1]);
