@@ -18,7 +18,7 @@
  *       (src/algorithm/physics/conservative_helmholtz.py:18-149) and the
  *       row scaling / Jacobi set-up of GpuIterativeSolver.solve
  *       (src/algorithm/solvers/iterative_solver.py:37-56).
- *   usv_operator_apply
+ *   usv_operator_apply / usv_operator_apply_kernel
  *       the CSR SpMV `A_gpu @ v` and its variants
  *       (iterative_solver.py:42,71,74-75; helmholtz_solver.py:613-620 for A^H).
  *   usv_gmres_workspace_bytes / usv_gmres_solve
@@ -26,6 +26,10 @@
  *       cupyx.scipy.sparse.linalg.gmres, as reached from
  *       HelmholtzDirectSolver._solve_iterative / _solve_gpu_adjoint
  *       (src/algorithm/solvers/helmholtz_solver.py:589-632).
+ *   usv_gmres_scenes_workspace_bytes / usv_gmres_solve_scenes
+ *       the same solve for the right-hand sides of several scenes at once
+ *       (the reference solves scenes one after the other; its column batching
+ *       of one scene is phase_response_basis.py:97-115).
  *   usv_materials_blend
  *       WarpAssemblyEngine material stage + blend_obstacle_material
  *       (src/algorithm/physics/warp_utils.py:11-23, 50-77).
@@ -136,17 +140,13 @@ typedef struct usv_gmres_params {
                                     streaming kernels (each CTA then loops over
                                     more node chunks); 0 = fill the GPU          */
     int32_t kernel_variant;      /* USV_GMRES_* bits; 0 = the measured-fastest
-                                    forms (bulk-copy orthogonalisation ring,
-                                    per-warp dot tasks)                          */
+                                    form (bulk-copy orthogonalisation ring)      */
 } usv_gmres_params;
 
 /* kernel_variant bits of usv_gmres_params (complex64 / bfloat16 vectors; the
- * complex128 path always uses the per-thread / per-warp forms) */
+ * complex128 path always uses the per-thread form) */
 #define USV_GMRES_ORTH_CPASYNC 1   /* orthogonalisation: per-thread cp.async
                                       pipeline instead of the bulk-copy ring  */
-#define USV_GMRES_DOTS_BULK 2      /* stencil + dots: bulk-copy tile ring with
-                                      per-warp node slices instead of per-warp
-                                      dot tasks with direct loads              */
 
 typedef struct usv_gmres_stats {
     int32_t status;              /* USV_OK or USV_ERR_*                          */

@@ -6,9 +6,9 @@ per-cycle host round trip dominate; many: the Krylov workspace grows as
 B (m+1) N and each RHS gets fewer CTAs). BatchTuner times a few restart
 cycles of the real operator at each candidate width that fits the memory
 budget and keeps the width with the lowest time per right-hand-side
-iteration; it then times the Arnoldi kernel forms at that width (the
-default, the per-thread cp.async orthogonalisation, the bulk-copy dot ring:
-usv_gmres_params.kernel_variant) and keeps the fastest. StencilTuner picks the complex64 operator-apply
+iteration; it then times the orthogonalisation kernel forms at that width
+(the bulk-copy ring or the per-thread cp.async pipeline:
+usv_gmres_params.kernel_variant) and keeps the faster. StencilTuner picks the complex64 operator-apply
 kernel (precomputed row coefficients, one thread per node, or 16-byte node
 records with z-marching tiles) for a grid and batch width. Results are cached
 in a JSON file keyed by GPU name, grid and the solver settings, so each
@@ -127,7 +127,7 @@ class BatchTuner:
         batch = rhs[idx]
         timings = {}
         try:
-            for variant in (0, N.GMRES_ORTH_CPASYNC, N.GMRES_DOTS_BULK):
+            for variant in (0, N.GMRES_ORTH_CPASYNC):
                 solver.kernel_variant = variant
                 solver.solve(operator, batch, adjoint=adjoint, raise_on_failure=False)
                 torch.cuda.synchronize(operator.device)

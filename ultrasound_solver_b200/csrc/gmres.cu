@@ -645,7 +645,12 @@ __device__ __forceinline__ void dots_finish(GState& g, int b, int j, bool proj, 
 // the extra launch and the re-read of w cost more than the overlap of the two
 // phases gains. Streaming the dots per thread through the cp.async pipeline
 // instead of warp tasks measured the same for bfloat16 and 8% slower for
-// complex64.)
+// complex64. Two bulk-copy forms of the dots were measured at 128^3 and
+// dropped: the chunk tiles of u_0 .. u_j through a cp.async.bulk ring with
+// every warp owning 1/16 of the chunk, 15% slower (a warp reduction per tile
+// and warp); each thread owning 8 nodes with its stencil in registers and
+// shared-memory partial sums, 1.7x slower (the stencil loads of 8 nodes per
+// thread at 25 warps per SM).)
 // mode 1 (recycled cycles): no stencil; the dots alpha_t = <C_t, r> of the
 // cycle's first residual r (slot kc) with the recycled C_t, t < kc.
 template <typename R, typename S, bool ADJ, int NT, bool MS = false>
@@ -804,208 +809,6 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         }
         part[t] = make_double2(re, im);
     }
-    if (!last_block_done(&g.counter[b], ncta)) return;
-    dots_finish(g, b, j, proj, ncta);
-}
-
-// Bulk-copy form of k_dots for bfloat16 vectors (USV_GMRES_DOTS_BULK), laid
-// out like k_orth_bulk: a CTA works on 2048-node chunks; each of the 256
-// consumer threads first forms w = sigma_j K u_j at its 8 nodes (stencil,
-// stored into the basis and kept in registers as packed bf16 words) while a
-// producer warp streams the chunk tiles of u_0 .. u_j through a 4-stage ring
-// of full / empty mbarriers (cp.async.bulk). Per tile every thread adds the
-// bf16 x bf16 products of its 8 nodes (fp32) to a partial sum in shared
-// memory that it shares with its neighbour lane (one shuffle), so no warp
-// reduction runs per tile; after the last chunk the CTA sums the partials of
-// each t in FP64 in a fixed order. ||w||^2 is summed while w is formed. All
-// waits are bounded (ST_DEVICE_TIMEOUT, then a bounded drain of the copies
-// in flight).
-struct DotsBulk {
-    static constexpr int LOG_STAGES = 2;
-    static constexpr int STAGES = 1 << LOG_STAGES;
-    static constexpr int TILE = kChunk * int(sizeof(bf2));  // bytes per chunk tile
-    static constexpr int THREADS = kThreads + 32;           // + the producer warp
-    static constexpr int SLOTS = kThreads / 2;              // partial sums per t
-    // ring, the fp32 partials of the m + 1 dots, barriers
-    static size_t smem(int m) {
-        return size_t(STAGES) * TILE + size_t(m + 1) * SLOTS * sizeof(float2) +
-               2 * STAGES * sizeof(unsigned long long);
-    }
-};
-
-template <typename R, bool ADJ, bool MS = false>
-__global__ void __launch_bounds__(DotsBulk::THREADS) k_dots_bulk(OpView<R> op, bf2* V, GState g,
-                                                                 int j, Step step, int mode) {
-    using P = DotsBulk;
-    const int b = blockIdx.y;
-    if (g.status[b] != ST_ACTIVE || g.ended[b]) return;
-    if constexpr (MS) op = slot_view<R>(g.slots[b]);
-    const int ncta = rhs_ctas<MS>(g, b);
-    if (int(blockIdx.x) >= ncta) return;
-    const CycleBasis<bf2> cb = cycle_basis(V, g, b);
-    const bool proj = mode == 1;
-    if (proj) {
-        if (cb.kc == 0) return;
-        j = cb.kc - 1;
-    } else if (j < cb.kc) {
-        return;
-    }
-    extern __shared__ __align__(128) char dyn[];
-    char* ring = dyn;
-    float2* psum = reinterpret_cast<float2*>(dyn + size_t(P::STAGES) * P::TILE);  // [m+1][SLOTS]
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(
-        reinterpret_cast<char*>(psum) + size_t(g.m + 1) * P::SLOTS * sizeof(float2));
-    unsigned long long* empty = full + P::STAGES;
-    __shared__ double sh[32];
-    __shared__ int failed;
-    const long long N = op.n;
-    const bf2* uj = cb.V + (long long)j * g.nv;
-    bf2* w = cb.V + (long long)(j + 1) * g.nv;
-    const R sj = R(g.sigma[b * (g.m + 1) + j]);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < (j + 1) * P::SLOTS; i += blockDim.x) psum[i] = make_float2(0.f, 0.f);
-    if (threadIdx.x == 0) {
-        failed = 0;
-        for (int st = 0; st < P::STAGES; ++st) {
-            mbar_init(&full[st], 1);
-            mbar_init(&empty[st], kThreads / 32);
-        }
-        mbar_fence_init();
-    }
-    __syncthreads();
-    const int nchunk = int((N + kChunk - 1) / kChunk);
-    const int nmy = nchunk > int(blockIdx.x) ? (nchunk - int(blockIdx.x) + ncta - 1) / ncta : 0;
-    const int tpc = j + 1;  // tiles per chunk: u_0 .. u_j
-    double wn = 0.0;        // ||w||^2 of this thread's nodes
-    if (warp == kThreads / 32) {
-        // producer: one elected thread issues the tiles of every chunk in order
-        if (lane == 0) {
-            int q = 0;
-            bool ok = true;
-            for (int i = 0; i < nmy && ok; ++i) {
-                const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * kChunk;
-                const int len = int(min((long long)kChunk, N - n0));
-                const unsigned bytes = unsigned((size_t(len) * sizeof(bf2) + 15) / 16 * 16);
-                for (int t = 0; t < tpc; ++t, ++q) {
-                    const int st = q & (P::STAGES - 1);
-                    if (!mbar_wait(&empty[st], (unsigned(q >> P::LOG_STAGES) & 1u) ^ 1u)) {
-                        ok = false;
-                        break;
-                    }
-                    const bf2* src = (t < cb.kc ? cb.C : cb.V) + (long long)t * g.nv + n0;
-                    mbar_expect_tx(&full[st], bytes);
-                    bulk_g2s(ring + size_t(st) * P::TILE, src, bytes, &full[st]);
-                }
-            }
-            if (!ok) {
-                failed = 1;
-                g.status[b] = ST_DEVICE_TIMEOUT;
-            }
-            for (int r = q > P::STAGES ? q - P::STAGES : 0; r < q; ++r)
-                mbar_wait(&full[r & (P::STAGES - 1)], unsigned(r >> P::LOG_STAGES) & 1u);
-        }
-    } else {
-        int q = 0;
-        bool ok = true;
-        for (int i = 0; i < nmy && ok; ++i) {
-            const long long n0 = (long long)(blockIdx.x + (long long)i * ncta) * kChunk;
-            const int len = int(min((long long)kChunk, N - n0));
-            // w at this thread's nodes: two units of 4 consecutive nodes
-            unsigned wv[8];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const int e0 = 4 * (threadIdx.x + kThreads * u);
-                unsigned wd[4];
-                if (mode == 0) {
-                    Node p = decode(n0 + e0, op.nx, op.ny);
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        bf2 y = from_d<bf2>(make_double2(0.0, 0.0));
-                        if (e0 + c < len)
-                            y = narrow<bf2>(cscale(k_row<R, ADJ, bf2>(op, uj, n0 + e0 + c, p), sj));
-                        wd[c] = *reinterpret_cast<const unsigned*>(&y);
-                        if (++p.i == op.nx) {
-                            p.i = 0;
-                            if (++p.j == op.ny) {
-                                p.j = 0;
-                                ++p.k;
-                            }
-                        }
-                    }
-                    if (e0 + 3 < len) {
-                        *reinterpret_cast<uint4*>(w + n0 + e0) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
-                    } else {
-                        for (int c = 0; c < 4 && e0 + c < len; ++c)
-                            reinterpret_cast<unsigned*>(w + n0 + e0)[c] = wd[c];
-                    }
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 4; ++c)
-                        wd[c] = e0 + c < len ? reinterpret_cast<const unsigned*>(w + n0 + e0)[c] : 0u;
-                }
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    wv[4 * u + c] = wd[c];
-                    const float2 f = bf2_to_f2(*reinterpret_cast<const bf2*>(&wd[c]));
-                    wn += double(f.x * f.x + f.y * f.y);
-                }
-            }
-            // dots of w with the chunk tiles of u_0 .. u_j; a unit that starts
-            // past len holds stale (possibly never written) shared memory, so
-            // it is replaced by zeros (a unit that starts before len was
-            // copied, rounded up into the zeroed padding of the vector)
-            const bool in0 = 4 * int(threadIdx.x) < len, in1 = 4 * int(threadIdx.x + kThreads) < len;
-            const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
-            for (int t = 0; t < tpc; ++t, ++q) {
-                const int st = q & (P::STAGES - 1);
-                if (!mbar_wait(&full[st], unsigned(q >> P::LOG_STAGES) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                const uint4* tile = reinterpret_cast<const uint4*>(ring + size_t(st) * P::TILE);
-                const uint4 a0 = in0 ? tile[threadIdx.x] : zero4;
-                const uint4 a1 = in1 ? tile[threadIdx.x + kThreads] : zero4;
-                float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
-                bf_mac(rr, ii, ri, ir, a0.x, wv[0]);
-                bf_mac(rr, ii, ri, ir, a0.y, wv[1]);
-                bf_mac(rr, ii, ri, ir, a0.z, wv[2]);
-                bf_mac(rr, ii, ri, ir, a0.w, wv[3]);
-                bf_mac(rr, ii, ri, ir, a1.x, wv[4]);
-                bf_mac(rr, ii, ri, ir, a1.y, wv[5]);
-                bf_mac(rr, ii, ri, ir, a1.z, wv[6]);
-                bf_mac(rr, ii, ri, ir, a1.w, wv[7]);
-                // the stage is released after its values have been used
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[st]);
-                float re = rr + ii, im = ri - ir;
-                re += __shfl_xor_sync(0xffffffffu, re, 1);
-                im += __shfl_xor_sync(0xffffffffu, im, 1);
-                if ((lane & 1) == 0) {
-                    float2& ps = psum[t * P::SLOTS + (threadIdx.x >> 1)];
-                    ps = make_float2(ps.x + re, ps.y + im);
-                }
-            }
-        }
-        if (!ok) {
-            failed = 1;
-            g.status[b] = ST_DEVICE_TIMEOUT;
-        }
-    }
-    wn = block_sum(wn, sh);  // (its barriers also make every partial visible)
-    if (failed) return;
-    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
-    for (int t = warp; t <= j; t += int(blockDim.x >> 5)) {
-        double re = 0.0, im = 0.0;
-        for (int sl = lane; sl < P::SLOTS; sl += 32) {
-            const float2 v = psum[t * P::SLOTS + sl];
-            re += double(v.x);
-            im += double(v.y);
-        }
-        const double v = warp_sum_pair(re, im);
-        if ((lane & 15) == 0)
-            reinterpret_cast<double*>(&part[t])[lane >> 4] = v * g.sigma[b * (g.m + 1) + t];
-    }
-    if (threadIdx.x == 0) part[j + 1] = make_double2(wn, 0.0);
     if (!last_block_done(&g.counter[b], ncta)) return;
     dots_finish(g, b, j, proj, ncta);
 }
@@ -2309,23 +2112,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     };
     dim3 grid_res, grid_dots, grid_orth, grid_upd, grid_gates;
     if (int e = grid_for((const void*)k_residual<ADJ, C2, MS>, 256, 0, grid_res)) return e;
-    // Arnoldi stencil + dots: per-warp dot tasks with direct loads (default;
-    // the bulk-copy tile ring of USV_GMRES_DOTS_BULK measured 15% slower at
-    // 128^3, its per-tile warp reductions cost more issue slots than the
-    // direct loads), always for complex128
-    const bool dots_warptask = (p.kernel_variant & USV_GMRES_DOTS_BULK) == 0;
-    const bool dots_bulk = !std::is_same<S, double2>::value && !dots_warptask;
-    const void* fn_dots = nullptr;
-    int dots_threads = kDotsThreads;
-    size_t dots_smem = 0;
-    if constexpr (std::is_same<S, bf2>::value) {
-        if (dots_bulk && DotsBulk::smem(g.m) <= 100 * 1024) {
-            fn_dots = (const void*)k_dots_bulk<R, ADJ, MS>;
-            dots_threads = DotsBulk::THREADS;
-            dots_smem = DotsBulk::smem(g.m);
-        }
-    }
-    if (!fn_dots) fn_dots = (const void*)k_dots<R, S, ADJ, kDotsThreads, MS>;
+    // Arnoldi stencil + dots: per-warp dot tasks with direct loads (two
+    // bulk-copy layouts measured slower at 128^3, see the dots kernel)
+    const void* fn_dots = (const void*)k_dots<R, S, ADJ, kDotsThreads, MS>;
+    const int dots_threads = kDotsThreads;
+    const size_t dots_smem = 0;
     USV_CUDA_TRY(cudaFuncSetAttribute(fn_dots, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(dots_smem)));
     if (int e = grid_for(fn_dots, dots_threads, dots_smem, grid_dots)) return e;
@@ -2749,7 +2540,7 @@ static int check_params(const usv_scene* scene, const usv_gmres_params* p, int n
         return USV_ERR_ARG;
     *m = int(p->restart < *n ? p->restart : *n);
     if (p->recycle < 0 || p->recycle_every < 0) return USV_ERR_ARG;
-    if (p->max_ctas < 0 || (p->kernel_variant & ~(USV_GMRES_ORTH_CPASYNC | USV_GMRES_DOTS_BULK)))
+    if (p->max_ctas < 0 || (p->kernel_variant & ~USV_GMRES_ORTH_CPASYNC))
         return USV_ERR_ARG;
     if (p->recycle > 0 && (p->recycle > kMaxRecycle || p->recycle > *m - 1)) return USV_ERR_ARG;
     *chunk = kChunk;  // node chunk per CTA (block_nodes is reserved)
