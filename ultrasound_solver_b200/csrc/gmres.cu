@@ -650,7 +650,12 @@ __device__ __forceinline__ void dots_finish(GState& g, int b, int j, bool proj, 
 // every warp owning 1/16 of the chunk, 15% slower (a warp reduction per tile
 // and warp); each thread owning 8 nodes with its stencil in registers and
 // shared-memory partial sums, 1.7x slower (the stencil loads of 8 nodes per
-// thread at 25 warps per SM).)
+// thread at 25 warps per SM). Also measured at 128^3 (4 RHS) and dropped:
+// one CTA per node chunk of all right-hand sides (row coefficients read once
+// per batch: faster at small j, slower at large j, 9% more dots time); a
+// bulk L2 prefetch of the next chunk's coefficient rows during the dots (5%
+// slower); segment counts balancing the dot tasks' load batches over the
+// warps (1% faster, but complex64 spilled).)
 // mode 1 (recycled cycles): no stencil; the dots alpha_t = <C_t, r> of the
 // cycle's first residual r (slot kc) with the recycled C_t, t < kc.
 template <typename R, typename S, bool ADJ, int NT, bool MS = false>
@@ -678,7 +683,12 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     // bfloat16: two chunks per phase (half the barriers, twice the loads in
     // flight per phase)
     constexpr int DC = std::is_same<C2, bf2>::value ? 2 * kChunk : kChunk;
-    __shared__ __align__(16) YS ys[DC];
+    // bfloat16: w of consecutive chunks alternates between two buffers, so a
+    // warp done with the dots of chunk c starts the stencil of chunk c+1 while
+    // others still read chunk c (one barrier per chunk, between the stencil
+    // and the dots)
+    constexpr int NBUF = std::is_same<C2, bf2>::value ? 2 : 1;
+    __shared__ __align__(16) YS ys_buf[NBUF][DC];
     __shared__ double2 segsum[USV_MAX_RESTART + 2 > NT / 16 ? USV_MAX_RESTART + 2 : NT / 16];
     const long long N = op.n;
     const C2* uj = cb.V + (long long)j * g.nv;
@@ -694,23 +704,44 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
     for (int task = threadIdx.x; task < tasks_t * segs; task += NT)
         segsum[task] = make_double2(0.0, 0.0);
     const int nphase = int((N + DC - 1) / DC);
-    for (int ch = blockIdx.x; ch < nphase; ch += ncta) {
+    for (int ch = blockIdx.x, par = 0; ch < nphase; ch += ncta, par ^= NBUF - 1) {
         const long long n0 = (long long)ch * DC;
         const int len = int(min((long long)DC, N - n0));
-        __syncthreads();  // the previous chunk's dots are done with ys
+        YS* ys = ys_buf[par];
+        // single buffer: the previous chunk's dots are done with ys. Double
+        // buffer: every warp passed the barrier below after its dots of the
+        // chunk before the previous one, the last reader of this buffer.
+        if (NBUF == 1) __syncthreads();
         if (mode == 0) {
-            Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
-            constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
-#pragma unroll(kStencilUnroll)
-            for (int e = threadIdx.x; e < DC; e += NT) {
-                C2 y = from_d<C2>(make_double2(0.0, 0.0));
-                if (e < len) {
-                    const long long n = n0 + e;
-                    y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
-                    w[n] = y;
+            if constexpr (std::is_same<C2, bf2>::value) {
+                // bfloat16 vectors: the complex64 coefficient rows without grid
+                // coordinates (the coefficient of a missing neighbour is zero,
+                // so its load only has to stay inside the vector: clamped
+                // index); 75 vs 84 us per launch at j = 0, 128^3, 4 RHS
+#pragma unroll 4
+                for (int e = threadIdx.x; e < DC; e += NT) {
+                    C2 y = from_d<C2>(make_double2(0.0, 0.0));
+                    if (e < len) {
+                        const long long n = n0 + e;
+                        y = narrow<C2>(cscale(k_row_cf_clamped(op, uj, n), sj));
+                        w[n] = y;
+                    }
+                    ys[e] = as_ys<YS>(y);
                 }
-                ys[e] = as_ys<YS>(y);
-                advance(p, step, op.nx, op.ny);
+            } else {
+                Node p = decode(n0 + threadIdx.x, op.nx, op.ny);
+                constexpr int kStencilUnroll = sizeof(R) == 4 ? 4 : 2;
+#pragma unroll(kStencilUnroll)
+                for (int e = threadIdx.x; e < DC; e += NT) {
+                    C2 y = from_d<C2>(make_double2(0.0, 0.0));
+                    if (e < len) {
+                        const long long n = n0 + e;
+                        y = narrow<C2>(cscale(k_row<R, ADJ, S>(op, uj, n, p), sj));
+                        w[n] = y;
+                    }
+                    ys[e] = as_ys<YS>(y);
+                    advance(p, step, op.nx, op.ny);
+                }
             }
         } else {
             for (int e = threadIdx.x; e < DC; e += NT)

@@ -411,6 +411,36 @@ __device__ __forceinline__ float2 k_row_cf(const OpView<float>& op, const S* __r
     return y;
 }
 
+// The same row without grid coordinates: a missing neighbour (zero
+// coefficient) is read at the neighbour index clamped into [0, N), a node of
+// the same vector. Equal to k_row_cf wherever u is finite (a zero coefficient
+// times a finite value adds zero).
+template <typename S>
+__device__ __forceinline__ float2 k_row_cf_clamped(const OpView<float>& op,
+                                                   const S* __restrict__ u, long long n) {
+    const float4* c = op.cf + 3 * n;
+    const float4 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2);
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny, last = op.n - 1;
+    const float2 u0 = widen<float2>(u[n > 0 ? n - 1 : 0]);
+    const float2 u1 = widen<float2>(u[n < last ? n + 1 : last]);
+    const float2 u2 = widen<float2>(u[n >= sy ? n - sy : 0]);
+    const float2 u3 = widen<float2>(u[n + sy <= last ? n + sy : last]);
+    const float2 u4 = widen<float2>(u[n >= sz ? n - sz : 0]);
+    const float2 u5 = widen<float2>(u[n + sz <= last ? n + sz : last]);
+    float2 y = widen<float2>(u[n]);
+    auto mac = [&](float cr, float ci, float2 v) {
+        y.x = fmaf(cr, v.x, fmaf(-ci, v.y, y.x));
+        y.y = fmaf(cr, v.y, fmaf(ci, v.x, y.y));
+    };
+    mac(c01.x, c01.y, u0);
+    mac(c01.z, c01.w, u1);
+    mac(c23.x, c23.y, u2);
+    mac(c23.z, c23.w, u3);
+    mac(c45.x, c45.y, u4);
+    mac(c45.z, c45.w, u5);
+    return y;
+}
+
 template <typename R, bool ADJ, typename S = typename Tr<R>::c2>
 __device__ __forceinline__ typename Tr<R>::c2 k_row(const OpView<R>& op, const S* __restrict__ u,
                                                     long long n, Node p) {
