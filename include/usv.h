@@ -147,6 +147,10 @@ typedef struct usv_gmres_params {
  * complex128 path always uses the per-thread form) */
 #define USV_GMRES_ORTH_CPASYNC 1   /* orthogonalisation: per-thread cp.async
                                       pipeline instead of the bulk-copy ring  */
+#define USV_GMRES_COMBINE_MMA_SYNC 2  /* bfloat16 GCRO-DR: the new recycled pair
+                                      with warp-level mma.sync instead of
+                                      tcgen05 (used in any case unless k is
+                                      4 or 8 and k + m + 1 <= 64)           */
 
 typedef struct usv_gmres_stats {
     int32_t status;              /* USV_OK or USV_ERR_*                          */

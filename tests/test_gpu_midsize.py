@@ -113,11 +113,11 @@ def test_fp64_iterations_independent_of_cta_cap(mid):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "bf16"])
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_arnoldi_kernel_variants(mid, precision, variant):
-    """Both orthogonalisation kernels (default: bulk-copy tile ring; the
-    per-thread cp.async pipeline) give the reference's solutions on the capped
-    grid, plain and recycled."""
+    """Every kernel form (orthogonalisation: bulk-copy tile ring or per-thread
+    cp.async pipeline; bfloat16 recycled pair: tcgen05 or mma.sync) gives the
+    reference's solutions on the capped grid, plain and recycled."""
     for algorithm in ("gmres30", "gcrodr36_8"):
         s = _solver(mid, precision, algorithm)
         s.iterative_solver.kernel_variant = variant
@@ -126,3 +126,32 @@ def test_arnoldi_kernel_variants(mid, precision, variant):
         G = mid["G"].astype(np.complex128)
         for k in range(3):
             assert rel(x[k], G[:, k]) <= TOL, (algorithm, k)
+
+
+@pytest.mark.parametrize("recycle", [4, 8])
+def test_recycled_pair_tensor_core_forms_agree(mid, recycle):
+    """bfloat16 GCRO-DR(36,k): the new recycled pair from tcgen05.mma (the
+    default for k = 4, 8) and from mma.sync (kernel_variant bit) both give the
+    reference's solutions, forward and adjoint, with the same iteration count
+    within a few restart cycles (the two products round differently)."""
+    from ultrasound_solver_b200 import _native as N
+    cols = None
+    counts = {}
+    for variant in (0, N.GMRES_COMBINE_MMA_SYNC):
+        s = golden_solver(mid, precision="bf16", gmres_rtol=1e-10, gmres_maxiter=200000,
+                          gmres_max_ctas=3, gmres_restart=36, gmres_recycle=recycle,
+                          gmres_recycle_every=2)
+        it = s.iterative_solver
+        it.kernel_variant = variant
+        if cols is None:
+            cols = s.sources.column_rhs(s.transducers.amplitudes)[:3]
+        x = it.solve(s.operator, cols).cpu().numpy()
+        counts[variant] = it.last_iterations
+        G = mid["G"].astype(np.complex128)
+        for k in range(3):
+            assert rel(x[k], G[:, k]) <= TOL, (variant, k)
+        rhs, sol = _adjoint_batch(mid, 2)
+        lam = it.solve(s.operator, torch.from_numpy(rhs.T.copy()).cuda(), adjoint=True)
+        for k in range(2):
+            assert rel(lam[k].cpu().numpy(), sol[:, k]) <= TOL, (variant, "adjoint", k)
+    assert abs(counts[0] - counts[N.GMRES_COMBINE_MMA_SYNC]) <= 4 * 36, counts

@@ -714,6 +714,7 @@ __global__ void __launch_bounds__(NT, 2) k_dots(OpView<R> op, S* V, GState g, in
         if (NBUF == 1) __syncthreads();
         if (mode == 0) {
             if constexpr (std::is_same<C2, bf2>::value) {
+                (void)step;
                 // bfloat16 vectors: the complex64 coefficient rows without grid
                 // coordinates (the coefficient of a missing neighbour is zero,
                 // so its load only has to stay inside the vector: clamped
@@ -1758,6 +1759,228 @@ __global__ void __launch_bounds__(kThreads) k_combine_mma(bf2* V, long long N, G
     if (threadIdx.x == 0) g.counter[b] = 0;
 }
 
+// The new recycled pair on the 5th-generation tensor cores (tcgen05.mma,
+// kind::f16, bf16 x bf16 -> fp32 accumulators in tensor memory), for
+// bfloat16 storage, K = 4 or 8 and at most kUmmaMaxRows input rows.
+// The product is arranged so that the packed {re, im} words of the input
+// vectors are an MN-major A operand as they lie in memory: a row of A is a
+// (node, part) pair, part = re / im, so 64 nodes give the M = 128 rows of
+// one MMA and a 16-byte piece of input vector r (4 nodes) is one row of a
+// canonical 8 x 16-byte core matrix (k = input row r). B (K-major, built once
+// per CTA) holds four real columns per complex output o: hi(c.re), lo(c.re),
+// hi(c.im), lo(c.im) of c = coef[r][o] (bf16 high part + remainder: 16
+// significant bits). Row (n, re) of D then holds sum_r v_r.re c_r, row (n, im)
+// sum_r v_r.im c_r, and lane pairs of the epilogue form
+//   out.re = P_re.re - P_im.im,  out.im = P_re.im + P_im.re.
+// Pipeline per CTA (128 threads): input tiles (rows x 64 nodes, 256 B per
+// row) reach shared memory by cp.async (16-byte pieces placed straight into
+// the core-matrix layout) through a kUmmaStages ring; thread 0 issues the
+// nks = ceil(rows / 16) MMAs of a tile into one of two TMEM accumulators and
+// commits them to that accumulator's mbarrier; all four warps read the
+// previous tile's accumulator (warp w: TMEM lanes 32w..32w+31), combine the
+// lane pairs, store U'_o / C'_o and sum ||U'_o||^2 from the stored values.
+// Every mbarrier wait is bounded; on a timeout the RHS ends with
+// ST_DEVICE_TIMEOUT and the CTA still waits (bounded) for its MMAs and frees
+// its tensor memory.
+constexpr int kUmmaThreads = 128;
+constexpr int kUmmaNodes = 64;      // nodes per tile: M = 128 rows (node, part)
+constexpr int kUmmaStages = 4;
+constexpr int kUmmaMaxRows = 64;    // input rows: at most 4 k-steps of 16
+constexpr size_t kUmmaMinSmem = 56 * 1024;  // <= 4 CTAs per SM: <= 512 TMEM columns
+__host__ __device__ constexpr int umma_tmem_cols(int k) { return 16 * k; }  // 2 x 8K, K = 4 or 8
+static size_t combine_umma_smem(int k, int m) {
+    const int nks = (k + m + 1 + 15) / 16;
+    const size_t need = size_t(kUmmaStages) * nks * 4096 + size_t(nks) * 16 * 8 * k * 2;
+    return need > kUmmaMinSmem ? need : kUmmaMinSmem;
+}
+template <int K, bool MS = false>
+__global__ void __launch_bounds__(kUmmaThreads) k_combine_umma(bf2* V, long long N, GState g) {
+    static_assert(K % 4 == 0 && K <= 8, "N = 8K columns: whole 32-column TMEM loads, <= 64");
+    constexpr int NC = 8 * K;  // real columns of B / D
+    constexpr int TC = umma_tmem_cols(K);
+    constexpr int S = kUmmaStages;
+    const int b = blockIdx.y;
+    if (g.status[b] != ST_ACTIVE) return;
+    if constexpr (MS) N = g.slots[b].n;
+    const int ncta = rhs_ctas<MS>(g, b);
+    if (int(blockIdx.x) >= ncta) return;
+    const int* cw = g.ctl + b * kCtl;
+    if (!cw[CW_COMBINE]) return;
+    const int m = g.m, skc = cw[CW_SRC_KC];
+    const int rows = skc + m + 1;  // <= kUmmaMaxRows (host)
+    const int nks = (rows + 15) / 16, nrg = (rows + 7) / 8;
+    const unsigned stage_bytes = unsigned(nks) * 4096u;
+    extern __shared__ __align__(128) unsigned char usm[];
+    unsigned char* As = usm;                                  // [S][2 nks][16][128 B]
+    unsigned char* Bs = usm + size_t(S) * stage_bytes;        // [2 nks][NC / 8][128 B]
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ unsigned tmem_s;
+    __shared__ double sh[kUmmaThreads / 32][K];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double2* coef = g.coef + (long long)b * (K + m + 1) * 2 * K;
+    // A stages zeroed once (rows past `rows` stay zero), B built in its core layout:
+    // element (k, n) at ((k / 8) (NC / 8) + n / 8) 128 + (n % 8) 16 + (k % 8) 2
+    for (unsigned q = tid; q < unsigned(S) * stage_bytes / 16; q += kUmmaThreads)
+        reinterpret_cast<uint4*>(As)[q] = make_uint4(0u, 0u, 0u, 0u);
+    for (int q = tid; q < 16 * nks * NC; q += kUmmaThreads) {
+        const int r = q / NC, col = q % NC, o = col >> 2, part = col & 3;
+        __nv_bfloat16 v = __float2bfloat16(0.f);
+        if (r < rows) {
+            const double2 c = coef[(long long)r * 2 * K + o];
+            const double x = part < 2 ? c.x : c.y;
+            const __nv_bfloat16 hi = __double2bfloat16(x);
+            v = (part & 1) ? __double2bfloat16(x - double(__bfloat162float(hi))) : hi;
+        }
+        *reinterpret_cast<__nv_bfloat16*>(Bs + (((r >> 3) * (NC / 8) + (col >> 3)) << 7) +
+                                          ((col & 7) << 4) + ((r & 7) << 1)) = v;
+    }
+    if (warp == 0) tmem_alloc(&tmem_s, TC);
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        mbar_fence_init();
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_s;
+
+    const long long sp = (cw[CW_SRC_PAIR] > 0 ? cw[CW_SRC_PAIR] : 0) * g.pstride + (long long)b * K * g.nv;
+    const long long dp = cw[CW_DST] * g.pstride + (long long)b * K * g.nv;
+    const unsigned* Uo = reinterpret_cast<const unsigned*>(static_cast<const bf2*>(g.Ubuf) + sp);
+    const unsigned* Co = reinterpret_cast<const unsigned*>(static_cast<const bf2*>(g.Cbuf) + sp);
+    unsigned* Un = reinterpret_cast<unsigned*>(static_cast<bf2*>(g.Ubuf) + dp);
+    unsigned* Cn = reinterpret_cast<unsigned*>(static_cast<bf2*>(g.Cbuf) + dp);
+    const unsigned* Vs = reinterpret_cast<const unsigned*>(V + cw[CW_SRC_VBUF] * g.vstride +
+                                                            (long long)b * (m + 1) * g.nv);
+    auto row = [&](int r) {
+        return r < skc ? Uo + (long long)r * g.nv
+                       : (r < 2 * skc ? Co + (long long)(r - skc) * g.nv : Vs + (long long)(r - skc) * g.nv);
+    };
+    __shared__ const unsigned* rowp[kUmmaMaxRows];
+    for (int r = tid; r < rows; r += kUmmaThreads) rowp[r] = row(r);
+    __syncthreads();
+    const long long ntile = (N + kUmmaNodes - 1) / kUmmaNodes;
+    const int my_tiles =
+        ntile > blockIdx.x ? int((ntile - 1 - blockIdx.x) / ncta + 1) : 0;
+    // tile t of this CTA: nodes [(blockIdx.x + t ncta) 64, +64), inside the
+    // zero-padded vectors (their length is a multiple of 64 nodes)
+    auto issue = [&](int t) {
+        if (t < my_tiles) {
+            const long long n0 = ((long long)blockIdx.x + (long long)t * ncta) * kUmmaNodes;
+            unsigned char* st = As + size_t(t % S) * stage_bytes;
+            for (int c = tid; c < nrg * 128; c += kUmmaThreads) {
+                const int r8 = c & 7, q = (c >> 3) & 15, rg = c >> 7, r = rg * 8 + r8;
+                if (r < rows) cp_async16(st + ((rg * 16 + q) << 7) + (r8 << 4), rowp[r] + n0 + 4 * q, 16);
+            }
+        }
+        cp_async_commit();
+    };
+    constexpr unsigned idesc = umma_idesc_bf16(128, NC, true, false);
+    const unsigned b_addr = smem_u32(Bs);
+    float nrm[K / 2];  // ||U'_o||^2 of this lane's outputs o = 2p + (lane & 1)
+#pragma unroll
+    for (int i = 0; i < K / 2; ++i) nrm[i] = 0.f;
+    bool ok = true;
+    int issued = 0;  // MMA groups committed (thread 0)
+#pragma unroll 1
+    for (int t = 0; t < S - 1; ++t) issue(t);
+#pragma unroll 1
+    for (int t = 0; t <= my_tiles; ++t) {
+        if (t < my_tiles) {
+            cp_async_wait<S - 2>();
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                const unsigned a_addr = smem_u32(As + size_t(t % S) * stage_bytes);
+                const unsigned d = tmem + unsigned(t & 1) * NC;
+                for (int ks = 0; ks < nks; ++ks)
+                    umma_bf16(d, umma_desc(a_addr + ks * 4096u, 2048u, 128u),
+                              umma_desc(b_addr + ks * 2u * NC * 16u, NC * 16u, 128u), idesc, ks > 0);
+                umma_commit(&mbar[t & 1]);
+                ++issued;
+            }
+        }
+        if (t >= 1) {
+            const int te = t - 1;
+            if (ok && !mbar_wait(&mbar[te & 1], unsigned(te >> 1) & 1u)) ok = false;
+            ok = __all_sync(0xffffffffu, ok);  // the TMEM loads below are warp-wide
+            tc_fence_after();
+            if (ok) {
+                const long long n0 = ((long long)blockIdx.x + (long long)te * ncta) * kUmmaNodes;
+                const long long node = n0 + 16 * warp + (lane >> 1);
+                const bool odd = (lane & 1) != 0;
+                const unsigned ta = tmem + (unsigned(32 * warp) << 16) + unsigned(te & 1) * NC;
+#pragma unroll
+                for (int h = 0; h < NC / 32; ++h) {
+                    float v[32];
+                    tmem_ld32(ta + 32u * h, v);
+                    // output pair (oe, oe + 1): the even lane (re row) forms
+                    // oe, the odd lane (im row) oe + 1; each sends its partner
+                    // the row's products for the partner's output
+#pragma unroll
+                    for (int jp = 0; jp < 4; ++jp) {
+                        const int oe = 8 * h + 2 * jp;
+                        const float ae = v[8 * jp] + v[8 * jp + 1], ce = v[8 * jp + 2] + v[8 * jp + 3];
+                        const float ao = v[8 * jp + 4] + v[8 * jp + 5], co = v[8 * jp + 6] + v[8 * jp + 7];
+                        const float pa = __shfl_xor_sync(0xffffffffu, odd ? ae : ao, 1);
+                        const float pc = __shfl_xor_sync(0xffffffffu, odd ? ce : co, 1);
+                        const float a = odd ? ao : ae, c = odd ? co : ce;
+                        const float re = odd ? pa - c : a - pc;
+                        const float im = odd ? pc + a : c + pa;
+                        if (node < N) {
+                            const bf2 wv = __floats2bfloat162_rn(re, im);
+                            unsigned* dst = (oe < K ? Un + (long long)oe * g.nv : Cn + (long long)(oe - K) * g.nv) +
+                                            (odd ? g.nv : 0);
+                            dst[node] = *reinterpret_cast<const unsigned*>(&wv);
+                            if (oe < K) {
+                                const float2 f = to_f(wv);
+                                nrm[oe >> 1] += f.x * f.x + f.y * f.y;
+                            }
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+        }
+        issue(t + S - 1);
+    }
+    cp_async_wait<0>();
+    if (!ok) {
+        g.status[b] = ST_DEVICE_TIMEOUT;
+        // MMAs still in flight must finish before their tensor memory is freed
+        if (tid == 0)
+            for (int r = issued > 2 ? issued - 2 : 0; r < issued; ++r)
+                mbar_wait(&mbar[r & 1], unsigned(r >> 1) & 1u);
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, TC);
+    // ||U'_o||^2 per CTA in a fixed order (lanes, then warps)
+#pragma unroll
+    for (int o = 0; o < K; ++o) {
+        const double t = warp_sum((lane & 1) == (o & 1) ? double(nrm[o >> 1]) : 0.0);
+        if (lane == 0) sh[warp][o] = t;
+    }
+    __syncthreads();
+    double2* part = g.partial + ((long long)b * g.nblk + blockIdx.x) * g.ps;
+    for (int o = tid; o < K; o += kUmmaThreads) {
+        double t = 0.0;
+        for (int w = 0; w < kUmmaThreads / 32; ++w) t += sh[w][o];
+        part[o] = make_double2(t, 0.0);
+    }
+    if (!last_block_done(&g.counter[b], ncta)) return;
+    for (int i = tid; i < K; i += kUmmaThreads) {
+        double t = 0.0;
+        const double2* pq = g.partial + (long long)b * g.nblk * g.ps + i;
+        for (int c = 0; c < ncta; ++c) t += ld_cg(pq + (long long)c * g.ps).x;
+        g.dU[((long long)cw[CW_DST] * gridDim.y + b) * K + i] = t > 0.0 ? 1.0 / sqrt(t) : 0.0;
+    }
+    if (tid == 0) g.counter[b] = 0;
+}
+
 // bd = Vhat^H Ut for bfloat16 storage on the tensor cores: D = A B with A
 // rows = the slots s <= m of Vhat (16 per row tile), k = (node, re/im), and
 // B columns {re, im} -> Re, {im, -re} -> Im of <Vhat_s, U_i> (exact bf16
@@ -2002,14 +2225,18 @@ struct EventHold {
 
 
 // The recycled-space kernels are instantiated for every k = 1..kMaxRecycle.
-template <typename S, int K, bool MS> const void* recycle_kernel_k(bool combine) {
-    if constexpr (std::is_same<S, bf2>::value)
+// (bfloat16: the new pair on tcgen05 when `umma` and k is 4 or 8, else mma.sync)
+template <typename S, int K, bool MS> const void* recycle_kernel_k(bool combine, bool umma) {
+    if constexpr (std::is_same<S, bf2>::value) {
+        if constexpr (K % 4 == 0 && K <= 8)
+            if (combine && umma) return (const void*)k_combine_umma<K, MS>;
         return combine ? (const void*)k_combine_mma<K, MS> : (const void*)k_bdots_mma<K, MS>;
+    }
     return combine ? (const void*)k_combine<S, K, MS> : (const void*)k_bdots<S, K, MS>;
 }
-template <typename S, bool MS> const void* recycle_kernel(int k, bool combine) {
+template <typename S, bool MS> const void* recycle_kernel(int k, bool combine, bool umma = false) {
     switch (k) {
-#define USV_K(K) case K: return recycle_kernel_k<S, K, MS>(combine);
+#define USV_K(K) case K: return recycle_kernel_k<S, K, MS>(combine, umma);
         USV_K(1) USV_K(2) USV_K(3) USV_K(4) USV_K(5) USV_K(6) USV_K(7) USV_K(8)
         USV_K(9) USV_K(10) USV_K(11) USV_K(12) USV_K(13) USV_K(14) USV_K(15) USV_K(16)
 #undef USV_K
@@ -2121,9 +2348,11 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     int dev = 0, sms = 0;
     USV_CUDA_TRY(cudaGetDevice(&dev));
     USV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    auto grid_for = [&](const void* fn, int threads, size_t smem, dim3& grid) -> int {
-        int per_sm = 0;
-        USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    auto grid_for = [&](const void* fn, int threads, size_t smem, dim3& grid,
+                        int fixed_per_sm = 0) -> int {
+        int per_sm = fixed_per_sm;
+        if (per_sm <= 0)
+            USV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
         // one wave of resident CTAs shared by the right-hand sides. For a
         // multi-scene batch the per-RHS shares are proportional to the scene
         // sizes (rhs_ctas) and add up to kSceneWaves waves while every RHS is
@@ -2187,22 +2416,49 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
     size_t bd_smem = 0, comb_smem = 0;
     const void* fn_bdots = nullptr;
     const void* fn_comb = nullptr;
+    bool comb_umma = false;
+    int comb_threads = kThreads;
     if (kr > 0) {
         using T = typename Wide<S>::T;
         bd_smem = std::is_same<S, bf2>::value
                       ? bdots_mma_smem(kr, g.m)
                       : sizeof(T) * size_t(kr) * kBdTile + sizeof(double2) * size_t(g.m + 1) * kr;
-        comb_smem = std::is_same<S, bf2>::value ? combine_mma_smem(kr, g.m)
-                                                : sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
+        // bfloat16, k = 4 or 8, k + m + 1 <= 64 input rows: the new pair on
+        // tcgen05 (USV_GMRES_COMBINE_MMA_SYNC keeps the mma.sync kernel)
+        comb_umma = std::is_same<S, bf2>::value && (kr == 4 || kr == 8) &&
+                    kr + g.m + 1 <= kUmmaMaxRows &&
+                    !(p.kernel_variant & USV_GMRES_COMBINE_MMA_SYNC);
+        comb_smem = comb_umma ? combine_umma_smem(kr, g.m)
+                    : std::is_same<S, bf2>::value ? combine_mma_smem(kr, g.m)
+                                                  : sizeof(T) * size_t(kr + g.m + 1) * 2 * kr;
+        comb_threads = comb_umma ? kUmmaThreads : kThreads;
         fn_bdots = recycle_kernel<S, MS>(kr, false);
-        fn_comb = recycle_kernel<S, MS>(kr, true);
+        fn_comb = recycle_kernel<S, MS>(kr, true, comb_umma);
         if (!fn_bdots || !fn_comb) return USV_ERR_ARG;
         USV_CUDA_TRY(cudaFuncSetAttribute(fn_bdots, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(bd_smem)));
         USV_CUDA_TRY(cudaFuncSetAttribute(fn_comb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           int(comb_smem)));
+        // the tcgen05 pair kernel holds ~57 KB per CTA: ask for the full
+        // shared-memory carveout so that three CTAs share an SM
+        if (comb_umma)
+            USV_CUDA_TRY(cudaFuncSetAttribute(fn_comb, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                              int(cudaSharedmemCarveoutMaxShared)));
         if (int e = grid_for(fn_bdots, kThreads, bd_smem, grid_bd)) return e;
-        if (int e = grid_for(fn_comb, kThreads, comb_smem, grid_comb)) return e;
+        // tcgen05 pair kernel: as many CTAs per SM as its shared memory allows
+        // (the occupancy query answers 1 for it), at most 512 TMEM columns
+        int comb_per_sm = 0;
+        if (comb_umma) {
+            int smem_sm = 0, smem_res = 0;
+            cudaFuncAttributes fa{};
+            USV_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+            USV_CUDA_TRY(cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+            USV_CUDA_TRY(cudaFuncGetAttributes(&fa, fn_comb));
+            comb_per_sm = int(size_t(smem_sm) / (comb_smem + fa.sharedSizeBytes + size_t(smem_res)));
+            const int by_tmem = 512 / umma_tmem_cols(kr);
+            comb_per_sm = comb_per_sm < 1 ? 1 : (comb_per_sm > by_tmem ? by_tmem : comb_per_sm);
+        }
+        if (int e = grid_for(fn_comb, comb_threads, comb_smem, grid_comb, comb_per_sm)) return e;
     }
     // zero the state and the solution
     USV_CUDA_TRY(cudaMemsetAsync(ws + L.state_begin, 0, L.total - L.state_begin, strm));
@@ -2285,7 +2541,7 @@ static int run_gmres(const usv_scene& s, const void* op_buf, const usv_gmres_par
                 GState gs = g;
                 long long nn_ = g.n;
                 void* args[] = {&vp, &nn_, &gs};
-                USV_CUDA_TRY(cudaLaunchKernel(fn_comb, grid_comb, dim3(kThreads), args, comb_smem, st));
+                USV_CUDA_TRY(cudaLaunchKernel(fn_comb, grid_comb, dim3(comb_threads), args, comb_smem, st));
             }
             USV_CUDA_TRY(mark(st, k++, capturing));
             fam.push_back(6);
@@ -2571,7 +2827,7 @@ static int check_params(const usv_scene* scene, const usv_gmres_params* p, int n
         return USV_ERR_ARG;
     *m = int(p->restart < *n ? p->restart : *n);
     if (p->recycle < 0 || p->recycle_every < 0) return USV_ERR_ARG;
-    if (p->max_ctas < 0 || (p->kernel_variant & ~USV_GMRES_ORTH_CPASYNC))
+    if (p->max_ctas < 0 || (p->kernel_variant & ~(USV_GMRES_ORTH_CPASYNC | USV_GMRES_COMBINE_MMA_SYNC)))
         return USV_ERR_ARG;
     if (p->recycle > 0 && (p->recycle > kMaxRecycle || p->recycle > *m - 1)) return USV_ERR_ARG;
     *chunk = kChunk;  // node chunk per CTA (block_nodes is reserved)

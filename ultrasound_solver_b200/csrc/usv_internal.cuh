@@ -695,6 +695,88 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
         : "memory");
 }
 
+// ---------------------------------------------------------------- tcgen05
+// 5th-generation tensor-core operations (sm_100a): tensor-memory (TMEM)
+// allocation, one-thread MMA issue with shared-memory operand descriptors,
+// completion on an mbarrier, and TMEM -> register loads. The descriptor and
+// instruction-descriptor bit layouts follow the PTX ISA's tcgen05 matrix
+// descriptors (the same fields as CUTLASS's UMMA::SmemDescriptor and
+// UMMA::InstrDescriptor).
+//
+// Shared-memory matrix descriptor, no swizzle: start address, leading-
+// dimension byte offset (LBO) and stride-dimension byte offset (SBO), each
+// >> 4 in 14 bits, version 1 (bits 46-47), layout type 0.
+__device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned lbo,
+                                                        unsigned sbo) {
+    return (unsigned long long)((saddr >> 4) & 0x3FFFu) |
+           ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16 with bf16 A and B, fp32 accumulator:
+// bit 4 D = f32, bits 7/10 A/B = bf16, bit 15 A MN-major (1) / K-major (0),
+// bit 16 the same for B, bits 17-22 N >> 3, bits 24-28 M >> 4.
+__host__ __device__ constexpr unsigned umma_idesc_bf16(int m, int n, bool a_mn, bool b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (unsigned(a_mn) << 15) | (unsigned(b_mn) << 16) |
+           (unsigned(n >> 3) << 17) | (unsigned(m >> 4) << 24);
+}
+// D[tmem] (+)= A B; accumulate = 0 overwrites D. Issued by one thread.
+__device__ __forceinline__ void umma_bf16(unsigned tmem_d, unsigned long long a,
+                                          unsigned long long b, unsigned idesc, int accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// Arrive (once) on `bar` when every MMA this thread issued before has completed.
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar))
+                 : "memory");
+}
+// One warp: allocate `ncols` TMEM columns (a power of two >= 32), address into *dst.
+__device__ __forceinline__ void tmem_alloc(unsigned* dst, unsigned ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(dst)), "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// generic-proxy shared-memory writes -> visible to the async proxy (MMA operands)
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 32 consecutive fp32 columns of this thread's TMEM lane (32x32b shape: warp
+// w % 4 reads lanes 32 (w % 4) .. +31), then wait for the load.
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32]) {
+    unsigned r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Status helpers shared by the translation units.
 int set_last_cuda_error(cudaError_t e);
 }  // namespace usv
