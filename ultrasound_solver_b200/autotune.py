@@ -6,9 +6,11 @@ per-cycle host round trip dominate; many: the Krylov workspace grows as
 B (m+1) N and each RHS gets fewer CTAs). BatchTuner times a few restart
 cycles of the real operator at each candidate width that fits the memory
 budget and keeps the width with the lowest time per right-hand-side
-iteration; it then times the orthogonalisation kernel forms at that width
-(the bulk-copy ring or the per-thread cp.async pipeline:
-usv_gmres_params.kernel_variant) and keeps the faster. StencilTuner picks the complex64 operator-apply
+iteration. It then times the kernel forms at that width
+(usv_gmres_params.kernel_variant) and keeps the fastest: the bulk-copy
+orthogonalisation ring or the per-thread cp.async pipeline and, with bf16
+GCRO-DR(m, 4 or 8), the recycled pair on tcgen05 or on mma.sync.
+StencilTuner picks the complex64 operator-apply
 kernel (precomputed row coefficients, one thread per node, or 16-byte node
 records with z-marching tiles) for a grid and batch width. Results are cached
 in a JSON file keyed by GPU name, grid and the solver settings, so each
@@ -127,7 +129,10 @@ class BatchTuner:
         batch = rhs[idx]
         timings = {}
         try:
-            for variant in (0, N.GMRES_ORTH_CPASYNC):
+            variants = [0, N.GMRES_ORTH_CPASYNC]
+            if solver.precision == "bf16" and solver.recycle in (4, 8):
+                variants.append(N.GMRES_COMBINE_MMA_SYNC)  # recycled pair: mma.sync form
+            for variant in variants:
                 solver.kernel_variant = variant
                 solver.solve(operator, batch, adjoint=adjoint, raise_on_failure=False)
                 torch.cuda.synchronize(operator.device)
