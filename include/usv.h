@@ -151,6 +151,9 @@ typedef struct usv_gmres_params {
                                       with warp-level mma.sync instead of
                                       tcgen05 (used in any case unless k is
                                       4 or 8 and k + m + 1 <= 64)           */
+#define USV_GMRES_DOTS_C64_ROWS 4  /* bfloat16 Arnoldi stencil: complex64 row
+                                      coefficients (48 B per node) instead
+                                      of packed bfloat16 ones (24 B)       */
 
 typedef struct usv_gmres_stats {
     int32_t status;              /* USV_OK or USV_ERR_*                          */

@@ -113,7 +113,7 @@ def test_fp64_iterations_independent_of_cta_cap(mid):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "bf16"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_arnoldi_kernel_variants(mid, precision, variant):
     """Every kernel form (orthogonalisation: bulk-copy tile ring or per-thread
     cp.async pipeline; bfloat16 recycled pair: tcgen05 or mma.sync) gives the

@@ -30,6 +30,7 @@ APPLY_A, APPLY_AH, APPLY_ABS_A, APPLY_ABS_AH, APPLY_K, APPLY_KH = range(6)
 PREC_FP64, PREC_MIXED, PREC_MIXED_BF16 = 0, 1, 2
 GMRES_ORTH_CPASYNC = 1
 GMRES_COMBINE_MMA_SYNC = 2
+GMRES_DOTS_C64_ROWS = 4
 STENCIL_AUTO, STENCIL_COEF_ROWS, STENCIL_RECORD_TILES = 0, 1, 2
 LOSS_FOCAL_PRESSURE, LOSS_FOCAL_CONTRAST, LOSS_CONTRAST_RATIO = 0, 1, 2
 

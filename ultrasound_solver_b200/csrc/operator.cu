@@ -214,11 +214,12 @@ __global__ void __launch_bounds__(256) k_edges(OpView<double> op, double2* e64) 
 
 // Complex64 row coefficients c_nd = R_n e_nd s_d (conj(e_nd) and the adjoint
 // scalings for K'), evaluated in FP64 by the same row code as the FP64
-// operator with a unit value in direction d only, then rounded once to fp32.
-// The complex64 rows (usv_internal.cuh: k_row_cf) then cost six complex
+// operator with a unit value in direction d only, then rounded once to fp32
+// (and, for the bfloat16 Arnoldi rows, to packed bfloat16 {re, im}). The
+// complex64 rows (usv_internal.cuh: k_row_cf) then cost six complex
 // multiply-adds per node.
 template <bool ADJ>
-__global__ void __launch_bounds__(256) k_coef(OpView<double> op, float4* cf) {
+__global__ void __launch_bounds__(256) k_coef(OpView<double> op, float4* cf, uint2* cb) {
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < op.n;
          n += (long long)gridDim.x * blockDim.x) {
         const Node p = decode(n, op.nx, op.ny);
@@ -234,6 +235,14 @@ __global__ void __launch_bounds__(256) k_coef(OpView<double> op, float4* cf) {
                 });
             c[d] = make_float2(float(v.x), float(v.y));
         }
+        unsigned pk[6];
+        for (int d = 0; d < 6; ++d) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(c[d].x, c[d].y);
+            pk[d] = *reinterpret_cast<const unsigned*>(&h);
+        }
+        cb[3 * n] = make_uint2(pk[0], pk[1]);
+        cb[3 * n + 1] = make_uint2(pk[2], pk[3]);
+        cb[3 * n + 2] = make_uint2(pk[4], pk[5]);
         cf[3 * n] = make_float4(c[0].x, c[0].y, c[1].x, c[1].y);
         cf[3 * n + 1] = make_float4(c[2].x, c[2].y, c[3].x, c[3].y);
         cf[3 * n + 2] = make_float4(c[4].x, c[4].y, c[5].x, c[5].y);
@@ -579,9 +588,11 @@ int usv_operator_build(const usv_scene* scene, const double* rho, const double* 
     k_edges<<<grid_for(a.op.n), 256, 0, strm>>>(a.op, reinterpret_cast<double2*>(buf + L.e64));
     USV_CUDA_TRY(cudaGetLastError());
     k_coef<false><<<grid_for(a.op.n), 256, 0, strm>>>(
-        make_view<double>(s, op_buf, false), reinterpret_cast<float4*>(buf + L.cf32f));
+        make_view<double>(s, op_buf, false), reinterpret_cast<float4*>(buf + L.cf32f),
+        reinterpret_cast<uint2*>(buf + L.cb16f));
     k_coef<true><<<grid_for(a.op.n), 256, 0, strm>>>(
-        make_view<double>(s, op_buf, true), reinterpret_cast<float4*>(buf + L.cf32a));
+        make_view<double>(s, op_buf, true), reinterpret_cast<float4*>(buf + L.cf32a),
+        reinterpret_cast<uint2*>(buf + L.cb16a));
     USV_CUDA_TRY(cudaGetLastError());
     int flag = 0;
     USV_CUDA_TRY(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, strm));

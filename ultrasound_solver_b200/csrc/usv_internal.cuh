@@ -149,7 +149,7 @@ __device__ __forceinline__ void bf_sq(float& rr, float& ii, unsigned y) {
 // so host and device agree without storing the layout itself.
 struct Layout {
     size_t tab64[3], q64[3], tab32[3], q32[3];
-    size_t rec64f, rec64a, d64, e64, rec32f, rec32a, cf32f, cf32a, flag;
+    size_t rec64f, rec64a, d64, e64, rec32f, rec32a, cf32f, cf32a, cb16f, cb16a, flag;
     size_t total;
 };
 
@@ -179,6 +179,10 @@ inline Layout make_layout(const usv_scene& s) {
     // directions, three float4 per node (forward, adjoint)
     L.cf32f = off;  off = align_up(off + 3 * sizeof(float4) * n);
     L.cf32a = off;  off = align_up(off + 3 * sizeof(float4) * n);
+    // the same coefficients in packed bfloat16 {re, im}, three uint2 per node
+    // (the bfloat16 Arnoldi rows: bf16 x bf16 products)
+    L.cb16f = off;  off = align_up(off + 3 * sizeof(uint2) * n);
+    L.cb16a = off;  off = align_up(off + 3 * sizeof(uint2) * n);
     L.flag = off;   off = align_up(off + 64);
     L.total = off;
     return L;
@@ -197,6 +201,7 @@ template <typename R> struct OpView {
     const C4* rec;          // {rho, R, s.re, s.im} (forward or adjoint)
     const double2* d;       // diagonal A_ii (fp64 path only)
     const float4* cf;       // complex64 path: row coefficients, 3 float4 per node
+    const uint2* cb;        // the same in packed bfloat16, 3 uint2 per node
     const double2* e64;     // FP64 edge coefficients of A, 6 per node
 };
 
@@ -224,6 +229,7 @@ inline OpView<R> make_view(const usv_scene& s, const void* buf, bool adjoint) {
     v.rec = reinterpret_cast<const typename OpView<R>::C4*>(b + rec);
     v.d = reinterpret_cast<const double2*>(b + L.d64);
     v.cf = dbl ? nullptr : reinterpret_cast<const float4*>(b + (adjoint ? L.cf32a : L.cf32f));
+    v.cb = dbl ? nullptr : reinterpret_cast<const uint2*>(b + (adjoint ? L.cb16a : L.cb16f));
     v.e64 = reinterpret_cast<const double2*>(b + L.e64);
     return v;
 }
@@ -439,6 +445,30 @@ __device__ __forceinline__ float2 k_row_cf_clamped(const OpView<float>& op,
     mac(c45.x, c45.y, u4);
     mac(c45.z, c45.w, u5);
     return y;
+}
+
+// The bfloat16 row from the packed bfloat16 coefficients: every product
+// c_d u_d is bf16 x bf16, exact in fp32 (fma.rn.f32.bf16), summed in fp32;
+// clamped neighbour indices as above.
+__device__ __forceinline__ float2 k_row_cb_clamped(const OpView<float>& op,
+                                                   const bf2* __restrict__ u, long long n) {
+    const uint2* c = op.cb + 3 * n;
+    const uint2 c01 = __ldg(c), c23 = __ldg(c + 1), c45 = __ldg(c + 2);
+    const long long sy = op.nx, sz = (long long)op.nx * op.ny, last = op.n - 1;
+    const unsigned* w = reinterpret_cast<const unsigned*>(u);
+    const unsigned u0 = w[n > 0 ? n - 1 : 0], u1 = w[n < last ? n + 1 : last];
+    const unsigned u2 = w[n >= sy ? n - sy : 0], u3 = w[n + sy <= last ? n + sy : last];
+    const unsigned u4 = w[n >= sz ? n - sz : 0], u5 = w[n + sz <= last ? n + sz : last];
+    // bf_mac accumulates conj(c) u: Re(c u) = rr - ii, Im(c u) = ri + ir
+    float rr = 0.f, ii = 0.f, ri = 0.f, ir = 0.f;
+    bf_mac(rr, ii, ri, ir, c01.x, u0);
+    bf_mac(rr, ii, ri, ir, c01.y, u1);
+    bf_mac(rr, ii, ri, ir, c23.x, u2);
+    bf_mac(rr, ii, ri, ir, c23.y, u3);
+    bf_mac(rr, ii, ri, ir, c45.x, u4);
+    bf_mac(rr, ii, ri, ir, c45.y, u5);
+    const float2 un = widen<float2>(u[n]);
+    return make_float2(un.x + (rr - ii), un.y + (ri + ir));
 }
 
 template <typename R, bool ADJ, typename S = typename Tr<R>::c2>
