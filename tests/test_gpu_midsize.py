@@ -116,8 +116,9 @@ def test_fp64_iterations_independent_of_cta_cap(mid):
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_arnoldi_kernel_variants(mid, precision, variant):
     """Every kernel form (orthogonalisation: bulk-copy tile ring or per-thread
-    cp.async pipeline; bfloat16 recycled pair: tcgen05 or mma.sync) gives the
-    reference's solutions on the capped grid, plain and recycled."""
+    cp.async pipeline; bfloat16 recycled pair: tcgen05 or mma.sync; bfloat16
+    stencil: packed-bf16 or complex64 row coefficients) gives the reference's
+    solutions on the capped grid, plain and recycled."""
     for algorithm in ("gmres30", "gcrodr36_8"):
         s = _solver(mid, precision, algorithm)
         s.iterative_solver.kernel_variant = variant
