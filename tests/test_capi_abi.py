@@ -145,3 +145,23 @@ def test_scene_batch_workspace_and_argument_checks(lib):
     tiny = (_native.Scene * 2)(scene(3), scene(12))  # 27 nodes < restart 30
     assert lib.usv_gmres_scenes_workspace_bytes(2, tiny, owner, ctypes.byref(p), 3,
                                                 ctypes.byref(nbytes)) == _native.USV_ERR_ARG
+
+
+def test_header_constants_match_the_python_layer():
+    """Every integer #define of include/usv.h has the same value in _native
+    (USV_ERR_* / USV_OK / USV_ABI_VERSION by their full name, the others by
+    the name after USV_)."""
+    import re
+    header = (build.INCLUDE / "usv.h").read_text()
+    seen = 0
+    for name, value in re.findall(r"^#define (USV_[A-Z0-9_]+) (\d+)", header, re.M):
+        if name == "USV_ABI_VERSION":
+            py = "ABI_VERSION"
+        elif name.startswith(("USV_ERR_", "USV_OK")):
+            py = name
+        else:
+            py = name[len("USV_"):]
+        assert hasattr(_native, py), f"{name} has no _native.{py}"
+        assert getattr(_native, py) == int(value), (name, getattr(_native, py), value)
+        seen += 1
+    assert seen >= 30
